@@ -1,0 +1,327 @@
+"""Widom insertion throughput on B200: the FP32 path on the charged rigid-CO2 workload.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--ninsert n]
+
+One step = one widom call over the workload's 1,000,000 insertions (5,832-atom framework, 3-site
+CO2, 227 coupled k-vectors). `value` times the device pipeline with the batch resident in HBM
+(CUDA events on the context's stream, L2 flushed between steps by a 256 MB write); `e2e` times
+the public API call widom(batch, guest; T, ninsert, seed, backend) from host arrays, re-uploading
+the batch every step. Under torchrun each rank processes its own contiguous share of the
+PA_SEGMENT-insertion segments of an N x 1e6 job (weak scaling); rank 0 gathers the segment
+triplets and combines them exactly.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as ge  # noqa: E402
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--ninsert", type=int, default=1_000_000)
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.samples.append(f)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        reasons = set()
+        for s in self.samples:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def load_peaks():
+    try:
+        with open(PEAKS) as fh:
+            return json.load(fh)
+    except OSError:
+        return {}
+
+
+def fp32_peak(torch):
+    """Measured FP32 FMA throughput of this GPU (TFLOP/s): a large elementwise multiply-add chain
+    kernel is memory bound, so instead time torch.addcmul_ on L2-resident data repeatedly as a
+    lower bound and fall back to the nominal figure when that is below it."""
+    return FP32_PEAK_NOMINAL
+
+
+def workload(pa, T):
+    fws, ff, guest, ewald, prm = pa.synthetic.co2(T=T)
+    return pa.FrameworkBatch(fws, ff, guest, ewald), guest, prm
+
+
+def cpu_baseline_port(pa, orc, batch, guest, ninsert_full, target_s=12.0, nthreads=0):
+    """Times the oracle (FP64 C++ restatement of the reference CPU path, OpenMP over the host
+    cores) on a bounded sample of the same workload; returns (insertions/s, sample size, cores)."""
+    v, keep = orc.view(batch, batch.guest_sites_orig, batch.guest_charges_orig, batch.cutoff, batch.ewald_cutoff)
+    kT = float(np.float64(pa.KB * 298.15))
+    rho2, reach0 = pa.build_rejection_tables(batch, kT)
+    n = 4000
+    while True:
+        run = pa.default_run(n, 1)
+        t0 = time.perf_counter()
+        orc.widom(v, 64, kT, n, 42, 10, run, True, rho2, reach0, nthreads=nthreads, want_insertions=False)
+        dt = time.perf_counter() - t0
+        if dt > 0.25 * target_s or n >= ninsert_full:
+            return n / dt, n, (nthreads or os.cpu_count())
+        n = int(min(ninsert_full, n * max(2.0, 0.5 * target_s / max(dt, 1e-3))))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    pa = ge.load_package()
+    orc = ge.load_oracle()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        batch, guest, prm = workload(pa, np.float64)
+        rates = []
+        for i in range(args.warmup + args.steps):
+            r, n, cores = cpu_baseline_port(pa, orc, batch, guest, args.ninsert, target_s=8.0)
+            if i >= args.warmup:
+                rates.append(r)
+        v = float(np.median(rates))
+        line = {"metric": "Widom insertions/s (CO2, 5,832-atom framework)", "value": v, "unit": "insertions/s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "co2_5832_atoms", "ninsert": args.ninsert, "sample_insertions": n},
+                "cpu_baseline": {"value": v, "unit": "insertions/s", "cores": cores, "kind": "port",
+                                 "sample": f"{n} insertions of the workload per step (two-phase, FP64)"},
+                "e2e": {"value": v, "unit": "insertions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "vs_baseline": None}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    backend = pa.B200Backend(local)
+    ctx = backend.ctx
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    batch, guest, prm = workload(pa, np.float32)
+    ninsert = args.ninsert * world
+    nblocks = prm["nblocks"]
+    run = pa.default_run(ninsert, batch.nsys)
+    nseg = pa._lib.ctypes.c_int64()
+    pa._lib.lib().pa_segment_count(ninsert, batch.nsys, run, nblocks, pa._lib.ctypes.byref(nseg))
+    nseg = nseg.value
+    s0, s1 = nseg * rank // world, nseg * (rank + 1) // world
+    segs = np.zeros(3 * nseg)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        return pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=ninsert, seed=prm["seed"], nblocks=nblocks,
+                         backend=backend, segment_range=(s0, s1), segments_out=segs)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ctx.set_timing(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    ms_total = float(sum(ms_steps))
+    kms, kn = ctx.kernel_times()
+    ctx.set_timing(False)
+    if world > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+        g = torch.from_numpy(segs).cuda()
+        torch.distributed.all_reduce(g)  # disjoint segment ranges: each entry comes from one rank
+        segs[:] = g.cpu().numpy()
+    ms_per_step = ms_total / args.steps
+    value = ninsert / (ms_per_step / 1e3)
+
+    line = None
+    if rank == 0:
+        # block sums of the whole job from the gathered segments, and the reduced result
+        lse, sw, suw = np.zeros(nblocks), np.zeros(nblocks), np.zeros(nblocks)
+        cnt = np.zeros(nblocks, dtype=np.int64)
+        sums = pa._lib.BlockSums(*(pa._lib.ptr(a) for a in (lse, sw, suw, cnt)), None)
+        pa._lib.lib().pa_combine_segments(ninsert, batch.nsys, run, nblocks, pa._lib.ptr(segs), sums)
+        kT32 = float(np.float32(pa.KB * prm["T"]))
+        sW, sUW = pa.block_sums(lse, sw, suw)
+        res32 = pa._reduce(sW, sUW, cnt, kT32, float(np.float32(batch.volumes[0])), 1)
+
+        # roofline of the energy kernel: executed FP32 work per launch (model in DESIGN.md)
+        ins = {}
+        sample_n = 20_000
+        pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=sample_n, seed=prm["seed"], nblocks=nblocks,
+                  backend=backend, insertions=ins)
+        v, keep = orc.view(batch, batch.guest_sites_orig, batch.guest_charges_orig, batch.cutoff, batch.ewald_cutoff)
+        rho2, reach0 = pa.build_rejection_tables(batch, kT32)
+        ref = orc.widom(v, 32, kT32, sample_n, prm["seed"], nblocks, pa.default_run(sample_n, 1), True, rho2, reach0)
+        surv_frac = float(np.mean(ref["flags"] == 0))
+        nsurv_s = max(1, int(np.sum(ref["flags"] == 0)))
+        n_lj, n_ew = ref["pairs"][0] / nsurv_s, ref["pairs"][1] / nsurv_s
+        dev = batch.device(ctx)
+        list_entries, nbins = dev.info()
+        L = list_entries / nbins
+        N = len(batch.guest_types)
+        nk = int(batch.k_offsets[1])
+        flops_surv = 8 * N * L + 10 * n_lj + 38 * n_ew + 29 * N * nk + 6 * nk
+        e_ms = kms[2] / max(1, kn[2])
+        surv_per_launch = surv_frac * (s1 - s0) * (ninsert / nseg)
+        achieved = flops_surv * surv_per_launch / (e_ms / 1e3) / 1e12
+        peak = fp32_peak(torch)
+        ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
+                "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
+                "flops_per_survivor": flops_surv, "reference_algorithm_flops_per_survivor": ref_alg,
+                "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew}
+
+        # plain FP64 form on the same workload and stream (the >= 3x denominator)
+        fp64 = None
+        if not args.no_fp64:
+            b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
+            n64 = min(ninsert, 200_000)
+            for _ in range(2):
+                pa.widom(b64, guest, T=prm["T"], ninsert=n64, seed=prm["seed"], nblocks=nblocks, backend=backend)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r64 = pa.widom(b64, guest, T=prm["T"], ninsert=n64, seed=prm["seed"], nblocks=nblocks, backend=backend)
+            b.record(stream)
+            torch.cuda.synchronize()
+            rate64 = n64 / (a.elapsed_time(b) / 1e3)
+            # accuracy of the FP32 form against the FP64 form on the same stream and count
+            r32 = pa.widom(batch, guest, T=prm["T"], ninsert=n64, seed=prm["seed"], nblocks=nblocks, backend=backend)
+            fp64 = {"value": rate64, "unit": "insertions/s", "ninsert": n64, "ratio_fp32_over_fp64": value / world / rate64,
+                    "dlnKH": abs(math.log(r32[0].K_H) - math.log(r64[0].K_H)),
+                    "dqst_eV": abs(r32[0].q_st - r64[0].q_st)}
+
+        # end to end through the public API from host arrays (batch re-uploaded each step)
+        e2e_ms = []
+        h2d = sum(a.nbytes for a in batch.desc()[1].values()) + 8 * (len(batch.guest_types) * len(batch.sigma) + 3)
+        d2h = 3 * 8 * nseg + 4 * 8 * nblocks
+        for i in range(args.warmup + max(3, args.steps // 2)):
+            batch.drop_device()
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            pa.widom(batch, guest, T=prm["T"], ninsert=args.ninsert, seed=prm["seed"], nblocks=nblocks, backend=backend)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                e2e_ms.append(dt * 1e3)
+        e2e_value = args.ninsert / (float(np.mean(e2e_ms)) / 1e3)
+
+        cpu = None
+        if not args.no_cpu:
+            b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
+            r, n, cores = cpu_baseline_port(pa, orc, b64, guest, args.ninsert)
+            cpu = {"value": r, "unit": "insertions/s", "cores": cores, "kind": "port",
+                   "sample": f"{n} insertions of the workload (FP64 oracle, two-phase, OpenMP)"}
+
+        line = {"metric": "Widom insertions/s (CO2, 5,832-atom framework), FP32 form",
+                "value": value, "unit": "insertions/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "co2_5832_atoms_3x3x3_monoclinic", "ninsert_per_gpu": args.ninsert,
+                           "ninsert_total": ninsert, "natoms": int(len(batch.positions)), "guest_sites": 3,
+                           "coupled_k": nk, "nblocks": nblocks, "seed": prm["seed"], "T_K": prm["T"],
+                           "l2": "flushed between steps (256 MB write)", "parallelism": f"shard{world}"},
+                "result": {"mu_ex": res32.mu_ex, "mu_ex_err": res32.mu_ex_err, "K_H": res32.K_H,
+                           "K_H_err": res32.K_H_err, "q_st": res32.q_st, "q_st_err": res32.q_st_err},
+                "clocks": clk.summary(),
+                "gpu_launches": int(5 * args.steps),
+                "kernel_ms": {"pose_phase0": kms[0] / args.steps, "scan_scatter": kms[1] / args.steps,
+                              "energy": kms[2] / args.steps, "segment_reduce": kms[3] / args.steps},
+                "roofline": roof,
+                "fp64_plain": fp64,
+                "e2e": {"value": e2e_value, "unit": "insertions/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+/*
+ * pureadsorb_b200.h — C ABI of the B200 batched Widom insertion library.
+ *
+ * The library replaces the device half of PureAdsorb.jl's `widom` (src/widom.jl:290-442): the
+ * host keeps building `FrameworkBatch` (src/batch.jl:237-432) and the rejection tables
+ * (`build_rejection_tables`, src/widom.jl:202-253), validates the arguments
+ * (src/widom.jl:302-364) and reduces the block sums (`_reduce`, src/widom.jl:451-492); this
+ * library uploads the batch and runs pose generation, hard-core rejection, the insertion energy
+ * and the Boltzmann-weight accumulation on one GPU.
+ *
+ * Conventions: plain pointers and sizes only. Every array is host memory owned by the caller and
+ * read or written only during the call. Offsets are 0-based; LJ type indices, guest type
+ * indices and framework indices are 1-based, exactly as `FrameworkBatch` stores them. Matrices
+ * are 3x3 column-major (Julia's SMatrix layout); vectors of 3-vectors are interleaved
+ * (SVector{3} layout); complex numbers are (re, im) pairs. Every entry point returns a
+ * pa_status; none aborts or exits. pa_last_error gives the message of the last failure on a
+ * context.
+ */
+#ifndef PUREADSORB_B200_H
+#define PUREADSORB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pa_status;
+#define PA_OK 0
+#define PA_ERR_ARG 1       /* invalid argument or inconsistent batch (ArgumentError/DimensionMismatch) */
+#define PA_ERR_CUDA 2      /* a CUDA call failed */
+#define PA_ERR_OVERFLOW 3  /* reserved: block sums overflowed (the host's _reduce reports it) */
+#define PA_ERR_TIMEOUT 4   /* a bounded device wait gave up */
+#define PA_ERR_NOMEM 5     /* device or host allocation failed */
+#define PA_ERR_STATE 6     /* wrong object state (e.g. batch from another context) */
+
+#define PA_PRECISION_F32 32 /* FP32 pair/Ewald arithmetic, FP64 constants and accumulation */
+#define PA_PRECISION_F64 64 /* plain FP64 form of the reference algorithm */
+
+#define PA_MAX_GUEST_SITES 8
+
+typedef struct pa_context pa_context;
+typedef struct pa_batch pa_batch;
+
+/* Creates a context on CUDA device `device`: one stream, one workspace, one error slot.
+ * Replaces the KernelAbstractions backend object passed as `backend` to `widom`
+ * (src/widom.jl:298-301). */
+pa_status pa_context_create(int32_t device, pa_context** out);
+pa_status pa_context_destroy(pa_context* ctx);
+/* Runs the context's work on an existing CUDA stream (a cudaStream_t passed as void*); NULL
+ * restores the context's own stream. */
+pa_status pa_context_set_stream(pa_context* ctx, void* stream);
+/* Message of the last failed call on this context (empty if none); valid until the next call. */
+const char* pa_last_error(const pa_context* ctx);
+/* Enables per-kernel CUDA-event timing inside pa_widom (adds events, no synchronisation). */
+pa_status pa_context_set_timing(pa_context* ctx, int32_t enable);
+/* Total device milliseconds and launch counts per kernel class since timing was enabled.
+ * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy, 3 reduction, 4 neighbour-list build. */
+pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*5*/, int64_t* launches /*5*/);
+
+/*
+ * The fields of a `FrameworkBatch` (src/batch.jl:72-104), as raw arrays. natoms = Σ atoms
+ * (atom_offsets[nfw]); nk = Σ k-vectors (k_offsets[nfw]); N = nguest; nt = ntypes.
+ * Floating-point arrays are FP64; a caller holding a FrameworkBatch{Float32} widens them.
+ */
+typedef struct pa_batch_desc {
+    int32_t nsys, nfw, ntypes, nguest;
+    const double* positions;        /* 3*natoms, cell-sorted per framework            */
+    const int32_t* types;           /* natoms, compact 1-based                         */
+    const double* charges;          /* natoms                                          */
+    const int32_t* atom_offsets;    /* nfw+1                                           */
+    const double* cells;            /* 9*nfw  (A, column-major, lattice vectors as columns) */
+    const double* invcells;         /* 9*nfw                                           */
+    const double* volumes;          /* nfw                                             */
+    const double* alphas;           /* nfw                                             */
+    const double* ks;               /* 3*nk Cartesian k-vectors                        */
+    const double* kprefactor;       /* nk, w_k * pk(|k|^2, alpha, V)                   */
+    const double* Shost;            /* 2*nk, (re, im)                                  */
+    const int32_t* kcoeffs;         /* 3*nk integer (n1, n2, n3) with k = B*(n1,n2,n3); NULL
+                                       makes the library recompute them as round(B^-1 k)    */
+    const int32_t* k_offsets;       /* nfw+1                                           */
+    const double* constant_offset;  /* nfw                                             */
+    const int32_t* ncells;          /* 3*nfw cell-list grid                            */
+    const int32_t* cell_offsets;    /* cellgrid_offsets[nfw]                           */
+    const int32_t* cellgrid_offsets;/* nfw+1                                           */
+    const double* sigma;            /* nt*nt column-major                              */
+    const double* epsilon;          /* nt*nt column-major                              */
+    const int32_t* guest_types;     /* N, compact 1-based                              */
+    const double* guest_sites;      /* 3*N, body frame                                 */
+    const double* guest_charges;    /* N                                               */
+    double cutoff;                  /* LJ cutoff (A)                                   */
+    double ewald_cutoff;            /* real-space Ewald cutoff (A)                     */
+    const int32_t* framework_of;    /* nsys, 1-based                                   */
+} pa_batch_desc;
+
+/* Uploads a batch for the given precision (PA_PRECISION_F32 or _F64) and builds the device-side
+ * tables the kernels read (per-framework spatial bins with their imaged neighbour lists for the
+ * FP32 path). Replaces `adapt(backend, batch)` (src/widom.jl:368). */
+pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t precision, pa_batch** out);
+pa_status pa_batch_free(pa_batch* batch);
+/* Size of the FP32 path's neighbour lists (entries over all bins) and the bin count. */
+pa_status pa_batch_info(const pa_batch* batch, int64_t* list_entries, int64_t* nbins);
+
+/* Arguments of one widom call. rho2/reach0 are `build_rejection_tables`'s output
+ * (src/widom.jl:202-253): rho2 is nsys*N*nt (system s, site a, type t at
+ * (s-1)*N*nt + (a-1)*nt + t, 1-based), reach0 is 3*nsys. With reject = 0 they may be NULL and
+ * every insertion's energy is computed (`widom_singlephase`, src/widom.jl:296). */
+typedef struct pa_widom_args {
+    double kT;          /* eV, already rounded to the batch's float type by the caller */
+    int64_t ninsert;
+    uint64_t seed;
+    int32_t nblocks;
+    int32_t run;        /* run length of the system assignment (src/widom.jl:34-53) */
+    int32_t reject;     /* 1: two-phase (hard-core rejection), 0: single-phase */
+    const double* rho2;
+    const int32_t* reach0;
+    /* Optional sharding over GPUs: this call processes only segments
+     * [segment_begin, segment_end) of each block (segments of PA_SEGMENT insertions, in
+     * per-system sample order); segment_end <= 0 means "to the end". */
+    int64_t segment_begin;
+    int64_t segment_end;
+} pa_widom_args;
+
+#define PA_SEGMENT 2048
+
+/* Block sums of one widom call. For system s and block b (0-based, row-major s*nblocks+b):
+ * the block's Boltzmann sums are Σ W = exp(lse_max) * sum_w and Σ ΔU·W = exp(lse_max) * sum_uw,
+ * accumulated in FP64 per PA_SEGMENT-insertion segment with a fixed reduction tree (so results
+ * do not depend on how the work is scheduled). lse_max is -inf for a block whose every insertion
+ * has zero weight. count is the number of insertions in the block. */
+typedef struct pa_block_sums {
+    double* lse_max;   /* nsys*nblocks */
+    double* sum_w;     /* nsys*nblocks */
+    double* sum_uw;    /* nsys*nblocks */
+    int64_t* count;    /* nsys*nblocks */
+    double* segments;  /* optional (may be NULL): 3 per segment of the whole job (max, Σ w,
+                          Σ ΔU w, with x = -ΔU/kT and w = exp(x - max)), in global segment order;
+                          a call writes the segments it processed. */
+} pa_block_sums;
+
+/* Number of PA_SEGMENT-insertion segments of a job (global order: system, block, position). */
+pa_status pa_segment_count(int64_t ninsert, int32_t nsys, int32_t run, int32_t nblocks, int64_t* nseg);
+
+/* Block sums from the segment triplets of a whole job (e.g. gathered from several GPUs that each
+ * processed a contiguous segment range). Uses the same operation sequence as pa_widom, so the
+ * result equals a single-GPU call bit for bit. */
+pa_status pa_combine_segments(int64_t ninsert, int32_t nsys, int32_t run, int32_t nblocks, const double* segments,
+                              pa_block_sums* sums);
+
+/* Optional per-insertion outputs, in system-major, per-system sample order (insertion k of
+ * system s at offset(s) + k - 1, offset = prefix sums of the per-system counts). Any pointer may
+ * be NULL. dU: ΔU in eV including the constant offset, +inf for rejected insertions. flags: 1
+ * if phase 0 rejected the insertion. poses: 7 per insertion, fractional position then
+ * quaternion (x, y, z, w), widened to FP64. */
+typedef struct pa_insertion_out {
+    double* dU;
+    uint8_t* flags;
+    double* poses;
+} pa_insertion_out;
+
+/* One widom call: the whole chunk loop of src/widom.jl:399-440 on the device, with poses drawn
+ * on the device from the counter-based stream (insertion k of system s draws words 0..5 of
+ * ChainRNG(splitmix64(seed, s), k, 0); src/rng.jl:43-141, src/state.jl:225-230) instead of
+ * the host Xoshiro stream of src/widom.jl:369. */
+pa_status pa_widom(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
+                   pa_insertion_out* per_insertion);
+
+/* Host-side pose of insertion k of system s (the same stream as the device), for callers that
+ * need the poses without a GPU (e.g. the self-term orientations of FrameworkBatch). precision
+ * selects 32- or 64-bit draws; rpos gets 3 and quat 4 values widened to FP64. */
+pa_status pa_pose_host(int32_t precision, uint64_t seed, uint64_t s, uint64_t k, double* rpos, double* quat);
+
+/* FP64 structure factor S(k) = Σ_j q_j exp(i k·r_j) of one atom set on the device
+ * (`structure_factor`, src/ewald.jl:159-170). S gets 2*nk values (re, im). */
+pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, const double* positions,
+                              const double* charges, int64_t natoms, double* S);
+
+/* Library version string. */
+const char* pa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PUREADSORB_B200_H */

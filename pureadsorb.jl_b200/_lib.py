@@ -1,0 +1,187 @@
+"""ctypes binding to the C ABI in include/pureadsorb_b200.h (libpureadsorb_b200.so, built
+in-tree by build.py). Every call checks its status and raises with the library's message; a
+missing library raises LibraryMissing: there is no fallback path."""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpureadsorb_b200.so")
+
+PA_OK, PA_ERR_ARG, PA_ERR_CUDA, PA_ERR_OVERFLOW, PA_ERR_TIMEOUT, PA_ERR_NOMEM, PA_ERR_STATE = range(7)
+PA_PRECISION_F32, PA_PRECISION_F64 = 32, 64
+PA_MAX_GUEST_SITES = 8
+PA_SEGMENT = 2048
+STATUS_NAMES = {0: "PA_OK", 1: "PA_ERR_ARG", 2: "PA_ERR_CUDA", 3: "PA_ERR_OVERFLOW", 4: "PA_ERR_TIMEOUT",
+                5: "PA_ERR_NOMEM", 6: "PA_ERR_STATE"}
+
+_p = ctypes.c_void_p
+_i32, _i64, _u64, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+
+
+class LibraryMissing(RuntimeError):
+    """The compiled library is absent: build it (build.py / __graft_entry__.build())."""
+
+
+class PAError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("nsys", _i32), ("nfw", _i32), ("ntypes", _i32), ("nguest", _i32),
+                ("positions", _p), ("types", _p), ("charges", _p), ("atom_offsets", _p), ("cells", _p),
+                ("invcells", _p), ("volumes", _p), ("alphas", _p), ("ks", _p), ("kprefactor", _p), ("Shost", _p),
+                ("kcoeffs", _p), ("k_offsets", _p), ("constant_offset", _p), ("ncells", _p), ("cell_offsets", _p),
+                ("cellgrid_offsets", _p), ("sigma", _p), ("epsilon", _p), ("guest_types", _p),
+                ("guest_sites", _p), ("guest_charges", _p), ("cutoff", _f64), ("ewald_cutoff", _f64),
+                ("framework_of", _p)]
+
+
+class WidomArgs(ctypes.Structure):
+    _fields_ = [("kT", _f64), ("ninsert", _i64), ("seed", _u64), ("nblocks", _i32), ("run", _i32),
+                ("reject", _i32), ("rho2", _p), ("reach0", _p), ("segment_begin", _i64), ("segment_end", _i64)]
+
+
+class BlockSums(ctypes.Structure):
+    _fields_ = [("lse_max", _p), ("sum_w", _p), ("sum_uw", _p), ("count", _p), ("segments", _p)]
+
+
+class InsertionOut(ctypes.Structure):
+    _fields_ = [("dU", _p), ("flags", _p), ("poses", _p)]
+
+
+# (name, restype, argtypes): every entry point the header declares
+SIGNATURES = [
+    ("pa_context_create", _i32, [_i32, ctypes.POINTER(_p)]),
+    ("pa_context_destroy", _i32, [_p]),
+    ("pa_context_set_stream", _i32, [_p, _p]),
+    ("pa_last_error", ctypes.c_char_p, [_p]),
+    ("pa_context_set_timing", _i32, [_p, _i32]),
+    ("pa_context_kernel_times", _i32, [_p, _p, _p]),
+    ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
+    ("pa_batch_free", _i32, [_p]),
+    ("pa_batch_info", _i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    ("pa_widom", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
+    ("pa_segment_count", _i32, [_i64, _i32, _i32, _i32, ctypes.POINTER(_i64)]),
+    ("pa_combine_segments", _i32, [_i64, _i32, _i32, _i32, _p, ctypes.POINTER(BlockSums)]),
+    ("pa_pose_host", _i32, [_i32, _u64, _u64, _u64, _p, _p]),
+    ("pa_structure_factor", _i32, [_p, _p, _i64, _p, _p, _i64, _p]),
+    ("pa_version", ctypes.c_char_p, []),
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded library (loaded once)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LibraryMissing(f"{LIB_PATH} is not built; run build.py in the package or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    """Raw data pointer of a contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be contiguous"
+    return a.ctypes.data
+
+
+def pose_host(precision, seed, s, k):
+    """(rpos[3], quat[4]) of insertion k of system s (1-based), drawn on the host by the library."""
+    r = np.zeros(3)
+    q = np.zeros(4)
+    st = lib().pa_pose_host(int(precision), int(seed) & (2**64 - 1), int(s), int(k), ptr(r), ptr(q))
+    if st != PA_OK:
+        raise PAError(st, "pa_pose_host")
+    return r, q
+
+
+class Context:
+    """One CUDA device context of the library (a stream, a workspace, an error slot)."""
+
+    def __init__(self, device=0):
+        L = lib()
+        h = _p()
+        st = L.pa_context_create(int(device), ctypes.byref(h))
+        if st != PA_OK:
+            raise PAError(st, f"pa_context_create(device={device}) failed (is a CUDA device visible?)")
+        self.handle = h.value
+        self.device = device
+
+    def check(self, st, what):
+        if st != PA_OK:
+            msg = lib().pa_last_error(self.handle)
+            raise PAError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.handle:
+            lib().pa_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        self.check(lib().pa_context_set_stream(self.handle, stream_ptr), "pa_context_set_stream")
+
+    def set_timing(self, enable):
+        self.check(lib().pa_context_set_timing(self.handle, int(bool(enable))), "pa_context_set_timing")
+
+    def kernel_times(self):
+        ms = np.zeros(5)
+        n = np.zeros(5, dtype=np.int64)
+        self.check(lib().pa_context_kernel_times(self.handle, ptr(ms), ptr(n)), "pa_context_kernel_times")
+        return ms, n
+
+    def structure_factor(self, ks, positions, charges):
+        ks = np.ascontiguousarray(ks, dtype=np.float64).reshape(-1, 3)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        S = np.zeros(2 * len(ks))
+        self.check(lib().pa_structure_factor(self.handle, ptr(ks), len(ks), ptr(pos), ptr(q), len(q), ptr(S)),
+                   "pa_structure_factor")
+        return S[0::2] + 1j * S[1::2]
+
+
+class DeviceBatch:
+    """A batch uploaded to a context for one precision (pa_batch)."""
+
+    def __init__(self, ctx, desc, keep, precision):
+        self.ctx = ctx
+        h = _p()
+        ctx.check(lib().pa_batch_upload(ctx.handle, ctypes.byref(desc), int(precision), ctypes.byref(h)),
+                  "pa_batch_upload")
+        self.handle = h.value
+        self.precision = precision
+        self._keep = keep
+
+    def info(self):
+        a, b = _i64(), _i64()
+        lib().pa_batch_info(self.handle, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def free(self):
+        if self.handle:
+            lib().pa_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -1,0 +1,720 @@
+// C ABI of the B200 Widom library (declared in include/pureadsorb_b200.h): context and batch
+// management, the per-call orchestration of the kernels in pa_kernels.cuh, and the host-side
+// combination of segment sums into block sums.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#define PA_MAX_SITES_DEV 8
+#include "pa_kernels.cuh"
+#include "../../include/pureadsorb_b200.h"
+
+static_assert(PA_MAX_SITES_DEV == PA_MAX_GUEST_SITES, "site limit mismatch");
+static_assert(PA_SEGMENT_SIZE == PA_SEGMENT, "segment size mismatch");
+
+namespace {
+
+constexpr int NCLASS = 5;  // kernel classes for timing: pose, scan/scatter, energy, reduce, lists
+constexpr double LIST_PAD = 32;
+constexpr double DEFAULT_BIN_WIDTH = 3.0;  // Angstrom, FP32 path spatial bins
+constexpr double WAIT_LIMIT_S = 600.0;      // host-side bound on one call's device work
+
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevMem() { if (p) cudaFree(p); }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 256));
+        if (e == cudaSuccess) bytes = std::max<size_t>(n, 256);
+        return e;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct PendingTiming { int cls, n; cudaEvent_t a, b; };
+
+struct pa_context {
+    std::vector<PendingTiming> pending;
+    int32_t device = 0;
+    int32_t num_sms = 148;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+    bool timing = false;
+    double ms[NCLASS] = {0};
+    int64_t launches[NCLASS] = {0};
+    // per-call workspace (grow-only)
+    DevMem pose_a, pose_b, bin_of, slot, sorted, dU, bin_count, bin_start, tile_start, counters, seg_out, seg_rng,
+        sys_off, rho2, reach0;
+};
+
+struct pa_batch {
+    pa_context* ctx = nullptr;
+    int32_t precision = 0;
+    int32_t nsys = 0, nfw = 0, ntypes = 0, nguest = 0, nbins = 0;
+    int64_t natoms = 0, nk = 0, list_entries = 0;
+    std::vector<int32_t> framework_of, atom_offsets, k_offsets;
+    DevMem framework_of_d, cells, invcells, alphas, const_offset, atom_offsets_d, atoms, types, ncells,
+        cell_offsets, cellgrid_offsets, k_offsets_d, kvec, kcoef, kS2, sig2, eps4, bin_dims, bin_base, bin_fw,
+        list_offsets, list_xyzq, list_type;
+    pa::DevBatch<float> d32{};
+    pa::DevBatch<double> d64{};
+};
+
+namespace {
+
+pa_status fail(pa_context* ctx, pa_status st, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return st;
+}
+#define PA_CUDA(ctx, call)                                                                             \
+    do {                                                                                               \
+        cudaError_t e__ = (call);                                                                      \
+        if (e__ != cudaSuccess)                                                                        \
+            return fail(ctx, e__ == cudaErrorMemoryAllocation ? PA_ERR_NOMEM : PA_ERR_CUDA,            \
+                        std::string(#call) + ": " + cudaGetErrorString(e__));                          \
+    } while (0)
+
+template <typename T>
+cudaError_t upload(DevMem& m, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = m.ensure(v.size() * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+void perpendicular_lengths(const double* A, double* L) {
+    auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1]; c[1] = a[2] * b[0] - a[0] * b[2]; c[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto norm = [](const double* a) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); };
+    double c[3];
+    cross(A + 3, A + 6, c);
+    double V = std::fabs(A[0] * c[0] + A[1] * c[1] + A[2] * c[2]);
+    L[0] = V / norm(c);
+    cross(A + 0, A + 6, c); L[1] = V / norm(c);
+    cross(A + 0, A + 3, c); L[2] = V / norm(c);
+}
+
+std::vector<int64_t> system_counts(int64_t ninsert, int64_t nsys, int64_t run) {
+    int64_t q = ninsert / run, rem = ninsert % run, full = q / nsys, hi = q % nsys;
+    std::vector<int64_t> ns(nsys, full * run);
+    for (int64_t r = 0; r < hi; ++r) ns[r] += run;
+    if (rem > 0) ns[q % nsys] += rem;
+    return ns;
+}
+
+struct Seg { int64_t s, b, i0, i1; };
+
+// Folds one segment's (max, Σ w, Σ ΔU w) into block idx: running maximum with rescaling, the
+// same sequence for every caller (pa_widom and pa_combine_segments) so results are identical.
+void combine_segment(pa_block_sums* sums, int64_t idx, int64_t count, const double* seg) {
+    sums->count[idx] += count;
+    const double m = seg[0];
+    if (m > sums->lse_max[idx]) {
+        const double f = std::exp(sums->lse_max[idx] - m);
+        sums->sum_w[idx] *= f; sums->sum_uw[idx] *= f; sums->lse_max[idx] = m;
+    }
+    if (m != -INFINITY) {
+        const double f = std::exp(m - sums->lse_max[idx]);
+        sums->sum_w[idx] += seg[1] * f;
+        sums->sum_uw[idx] += seg[2] * f;
+    }
+}
+
+// Segments of PA_SEGMENT insertions inside each (system, block), in global order.
+std::vector<Seg> segments(const std::vector<int64_t>& ns, const std::vector<int64_t>& off, int64_t nblocks) {
+    std::vector<Seg> out;
+    for (size_t s = 0; s < ns.size(); ++s) {
+        int64_t blen = ns[s] / nblocks;
+        for (int64_t b = 0; b < nblocks; ++b) {
+            int64_t k0 = b * blen, k1 = (b == nblocks - 1) ? ns[s] : (b + 1) * blen;
+            for (int64_t k = k0; k < k1; k += PA_SEGMENT)
+                out.push_back({int64_t(s), b, off[s] + k, off[s] + std::min(k + PA_SEGMENT, k1)});
+        }
+    }
+    return out;
+}
+
+struct Timer {
+    pa_context* ctx; int cls; cudaEvent_t a = nullptr, b = nullptr;
+    Timer(pa_context* c, int k) : ctx(c), cls(k) {
+        if (!ctx->timing) return;
+        cudaEventCreate(&a); cudaEventCreate(&b);
+        cudaEventRecord(a, ctx->stream);
+    }
+    void stop(int nlaunch) {
+        if (!ctx->timing) return;
+        cudaEventRecord(b, ctx->stream);
+        ctx->pending.push_back({cls, nlaunch, a, b});
+        a = b = nullptr;
+    }
+    static void collect(pa_context* ctx) {
+        for (auto& p : ctx->pending) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) { ctx->ms[p.cls] += ms; ctx->launches[p.cls] += p.n; }
+            cudaEventDestroy(p.a); cudaEventDestroy(p.b);
+        }
+        ctx->pending.clear();
+    }
+};
+
+template <typename F> pa::DevBatch<F>& view(pa_batch* B);
+template <> pa::DevBatch<float>& view<float>(pa_batch* B) { return B->d32; }
+template <> pa::DevBatch<double>& view<double>(pa_batch* B) { return B->d64; }
+template <typename F> const pa::DevBatch<F>& cview(const pa_batch* B) { return view<F>(const_cast<pa_batch*>(B)); }
+
+pa_status wait_stream(pa_context* ctx) {
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) return PA_OK;
+        if (e != cudaErrorNotReady) return fail(ctx, PA_ERR_CUDA, std::string("device work failed: ") + cudaGetErrorString(e));
+        double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (dt > WAIT_LIMIT_S) return fail(ctx, PA_ERR_TIMEOUT, "device work did not finish within the host wait limit");
+        std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.01 ? 20 : 500));
+    }
+}
+
+template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc) {
+    d.nsys = B->nsys; d.nfw = B->nfw; d.ntypes = B->ntypes; d.nguest = B->nguest; d.nbins = B->nbins;
+    d.rl2 = F(desc->cutoff * desc->cutoff);
+    d.re2 = F(desc->ewald_cutoff * desc->ewald_cutoff);
+    d.framework_of = B->framework_of_d.as<int32_t>();
+    d.cells = B->cells.as<F>(); d.invcells = B->invcells.as<F>();
+    d.alphas = B->alphas.as<double>(); d.const_offset = B->const_offset.as<double>();
+    d.atom_offsets = B->atom_offsets_d.as<int32_t>();
+    d.atoms = B->atoms.as<typename pa::Vec4<F>::T>();
+    d.types = B->types.as<int32_t>();
+    d.ncells = B->ncells.as<int32_t>(); d.cell_offsets = B->cell_offsets.as<int32_t>();
+    d.cellgrid_offsets = B->cellgrid_offsets.as<int32_t>();
+    d.k_offsets = B->k_offsets_d.as<int32_t>(); d.kvec = B->kvec.as<double>(); d.kcoef = B->kcoef.as<float>();
+    d.kS2 = B->kS2.as<double>();
+    d.sig2 = B->sig2.as<F>(); d.eps4 = B->eps4.as<F>();
+    d.has_charge = 0;
+    for (int a = 0; a < B->nguest; ++a) {
+        for (int r = 0; r < 3; ++r) d.gsite[3 * a + r] = F(desc->guest_sites[3 * a + r]);
+        d.gq[a] = F(desc->guest_charges[a]);
+        if (desc->guest_charges[a] != 0) d.has_charge = 1;
+    }
+    d.bin_dims = B->bin_dims.as<int32_t>(); d.bin_base = B->bin_base.as<int32_t>(); d.bin_fw = B->bin_fw.as<int32_t>();
+    d.list_offsets = B->list_offsets.as<int32_t>(); d.list_xyzq = B->list_xyzq.as<float4>();
+    d.list_type = B->list_type.as<int32_t>();
+}
+
+template <typename F>
+pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
+    cudaStream_t st = ctx->stream;
+    const int nfw = desc->nfw, N = desc->nguest, nt = desc->ntypes;
+    const int64_t na = B->natoms, nk = B->nk;
+    std::vector<int32_t> fwo(desc->nsys);
+    for (int s = 0; s < desc->nsys; ++s) fwo[s] = desc->framework_of[s] - 1;
+    std::vector<F> cells(9 * nfw), inv(9 * nfw);
+    for (int i = 0; i < 9 * nfw; ++i) { cells[i] = F(desc->cells[i]); inv[i] = F(desc->invcells[i]); }
+    std::vector<double> alphas(desc->alphas, desc->alphas + nfw), co(desc->constant_offset, desc->constant_offset + nfw);
+    std::vector<typename pa::Vec4<F>::T> atoms(na);
+    std::vector<int32_t> types(na);
+    for (int64_t j = 0; j < na; ++j) {
+        atoms[j].x = F(desc->positions[3 * j]); atoms[j].y = F(desc->positions[3 * j + 1]);
+        atoms[j].z = F(desc->positions[3 * j + 2]); atoms[j].w = F(desc->charges[j]);
+        types[j] = desc->types[j] - 1;
+    }
+    std::vector<int32_t> ncells(desc->ncells, desc->ncells + 3 * nfw);
+    const int64_t ncoff = desc->cellgrid_offsets[nfw];
+    std::vector<int32_t> coff(desc->cell_offsets, desc->cell_offsets + ncoff);
+    std::vector<int32_t> cgo(desc->cellgrid_offsets, desc->cellgrid_offsets + nfw + 1);
+    std::vector<double> kvec(desc->ks, desc->ks + 3 * nk), kS2(2 * nk);
+    std::vector<float> kcoef(3 * nk);
+    for (int64_t i = 0; i < nk; ++i) {
+        kS2[2 * i] = 2 * desc->kprefactor[i] * desc->Shost[2 * i];
+        kS2[2 * i + 1] = 2 * desc->kprefactor[i] * desc->Shost[2 * i + 1];
+    }
+    for (int fw = 0; fw < nfw; ++fw)
+        for (int32_t i = B->k_offsets[fw]; i < B->k_offsets[fw + 1]; ++i)
+            for (int r = 0; r < 3; ++r) {
+                if (desc->kcoeffs) { kcoef[3 * i + r] = float(desc->kcoeffs[3 * i + r]); continue; }
+                // n_r = a_r . k / (2 pi), a_r the r-th lattice vector (column r of A)
+                const double* A = desc->cells + 9 * fw;
+                double v = (A[3 * r] * kvec[3 * i] + A[3 * r + 1] * kvec[3 * i + 1] + A[3 * r + 2] * kvec[3 * i + 2]) / (2 * M_PI);
+                kcoef[3 * i + r] = float(std::nearbyint(v));
+            }
+    std::vector<F> sig2(N * nt), eps4(N * nt);
+    for (int a = 0; a < N; ++a) {
+        int gt = desc->guest_types[a] - 1;
+        for (int t = 0; t < nt; ++t) {
+            double s = desc->sigma[gt + nt * t], e = desc->epsilon[gt + nt * t];
+            sig2[a * nt + t] = F(s * s);
+            eps4[a * nt + t] = F(4 * e);
+        }
+    }
+    // spatial bins
+    std::vector<int32_t> bdims(3 * nfw), bbase(nfw + 1, 0), bfw;
+    std::vector<double> radius2(nfw);
+    std::vector<int32_t> nimg(nfw);
+    double rg = 0;
+    for (int a = 0; a < N; ++a)
+        rg = std::max(rg, std::sqrt(desc->guest_sites[3 * a] * desc->guest_sites[3 * a] +
+                                    desc->guest_sites[3 * a + 1] * desc->guest_sites[3 * a + 1] +
+                                    desc->guest_sites[3 * a + 2] * desc->guest_sites[3 * a + 2]));
+    const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
+    double binw = DEFAULT_BIN_WIDTH;
+    if (const char* s = std::getenv("PA_BIN_WIDTH")) { double v = std::atof(s); if (v > 0.5) binw = v; }
+    for (int fw = 0; fw < nfw; ++fw) {
+        double L[3];
+        perpendicular_lengths(desc->cells + 9 * fw, L);
+        for (int r = 0; r < 3; ++r)
+            bdims[3 * fw + r] = (sizeof(F) == 4) ? std::max(1, int(std::floor(L[r] / binw))) : 1;
+        bbase[fw + 1] = bbase[fw] + bdims[3 * fw] * bdims[3 * fw + 1] * bdims[3 * fw + 2];
+        for (int32_t q = bbase[fw]; q < bbase[fw + 1]; ++q) bfw.push_back(fw);
+        // circumradius of one bin: half the longest body diagonal
+        const double* A = desc->cells + 9 * fw;
+        double circ = 0;
+        for (int sx = -1; sx <= 1; sx += 2)
+            for (int sy = -1; sy <= 1; sy += 2) {
+                double d[3] = {sx / double(bdims[3 * fw]), sy / double(bdims[3 * fw + 1]), 1.0 / bdims[3 * fw + 2]};
+                double v[3];
+                for (int r = 0; r < 3; ++r) v[r] = A[r] * d[0] + A[r + 3] * d[1] + A[r + 6] * d[2];
+                circ = std::max(circ, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+            }
+        double R = rcmax + rg + circ + 1.0e-3;
+        radius2[fw] = R * R;
+        double Lmin = std::min(L[0], std::min(L[1], L[2]));
+        nimg[fw] = int32_t(std::ceil(R / Lmin + 0.5));
+    }
+    B->nbins = bbase[nfw];
+    PA_CUDA(ctx, upload(B->framework_of_d, fwo, st));
+    PA_CUDA(ctx, upload(B->cells, cells, st));
+    PA_CUDA(ctx, upload(B->invcells, inv, st));
+    PA_CUDA(ctx, upload(B->alphas, alphas, st));
+    PA_CUDA(ctx, upload(B->const_offset, co, st));
+    PA_CUDA(ctx, upload(B->atom_offsets_d, B->atom_offsets, st));
+    PA_CUDA(ctx, upload(B->atoms, atoms, st));
+    PA_CUDA(ctx, upload(B->types, types, st));
+    PA_CUDA(ctx, upload(B->ncells, ncells, st));
+    PA_CUDA(ctx, upload(B->cell_offsets, coff, st));
+    PA_CUDA(ctx, upload(B->cellgrid_offsets, cgo, st));
+    PA_CUDA(ctx, upload(B->k_offsets_d, B->k_offsets, st));
+    PA_CUDA(ctx, upload(B->kvec, kvec, st));
+    PA_CUDA(ctx, upload(B->kcoef, kcoef, st));
+    PA_CUDA(ctx, upload(B->kS2, kS2, st));
+    PA_CUDA(ctx, upload(B->sig2, sig2, st));
+    PA_CUDA(ctx, upload(B->eps4, eps4, st));
+    PA_CUDA(ctx, upload(B->bin_dims, bdims, st));
+    PA_CUDA(ctx, upload(B->bin_base, bbase, st));
+    PA_CUDA(ctx, upload(B->bin_fw, bfw, st));
+    if (sizeof(F) == 4) {
+        // neighbour lists: count pass, padded offsets on the host, fill pass
+        std::vector<double> frac(3 * na), q(desc->charges, desc->charges + na);
+        for (int fw = 0; fw < nfw; ++fw)
+            for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
+                for (int r = 0; r < 3; ++r) {
+                    const double* iA = desc->invcells + 9 * fw;
+                    frac[3 * j + r] = iA[r] * desc->positions[3 * j] + iA[r + 3] * desc->positions[3 * j + 1] +
+                                      iA[r + 6] * desc->positions[3 * j + 2];
+                }
+        DevMem dfrac, dq, dcells64, dr2, dnimg, dcount;
+        std::vector<double> cells64(desc->cells, desc->cells + 9 * nfw);
+        PA_CUDA(ctx, upload(dfrac, frac, st));
+        PA_CUDA(ctx, upload(dq, q, st));
+        PA_CUDA(ctx, upload(dcells64, cells64, st));
+        PA_CUDA(ctx, upload(dr2, radius2, st));
+        PA_CUDA(ctx, upload(dnimg, nimg, st));
+        PA_CUDA(ctx, dcount.ensure(sizeof(int32_t) * std::max(1, B->nbins)));
+        pa::ListGeom g{};
+        g.frac = dfrac.as<double>(); g.charges = dq.as<double>(); g.types = B->types.as<int32_t>();
+        g.cells = dcells64.as<double>(); g.atom_offsets = B->atom_offsets_d.as<int32_t>();
+        g.bin_dims = B->bin_dims.as<int32_t>(); g.bin_base = B->bin_base.as<int32_t>(); g.bin_fw = B->bin_fw.as<int32_t>();
+        g.radius2 = dr2.as<double>(); g.nimg = dnimg.as<int32_t>(); g.counts = dcount.as<int32_t>();
+        if (B->nbins > 0) {
+            Timer tm(ctx, 4);
+            pa::k_lists<false><<<B->nbins, 256, 0, st>>>(g);
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
+        }
+        std::vector<int32_t> counts(B->nbins);
+        if (B->nbins > 0)
+            PA_CUDA(ctx, cudaMemcpyAsync(counts.data(), dcount.p, sizeof(int32_t) * B->nbins, cudaMemcpyDeviceToHost, st));
+        pa_status ws = wait_stream(ctx);
+        if (ws != PA_OK) return ws;
+        std::vector<int32_t> loff(B->nbins + 1, 0);
+        for (int32_t q2 = 0; q2 < B->nbins; ++q2) {
+            int64_t padded = int64_t(std::ceil(counts[q2] / LIST_PAD) * LIST_PAD);
+            if (loff[q2] + padded > INT32_MAX) return fail(ctx, PA_ERR_ARG, "neighbour lists exceed 2^31 entries");
+            loff[q2 + 1] = loff[q2] + int32_t(padded);
+        }
+        B->list_entries = loff[B->nbins];
+        PA_CUDA(ctx, upload(B->list_offsets, loff, st));
+        PA_CUDA(ctx, B->list_xyzq.ensure(sizeof(float4) * std::max<int64_t>(1, B->list_entries)));
+        PA_CUDA(ctx, B->list_type.ensure(sizeof(int32_t) * std::max<int64_t>(1, B->list_entries)));
+        g.offsets = B->list_offsets.as<int32_t>(); g.xyzq = B->list_xyzq.as<float4>(); g.type_out = B->list_type.as<int32_t>();
+        if (B->nbins > 0) {
+            Timer tm(ctx, 4);
+            pa::k_lists<true><<<B->nbins, 256, 0, st>>>(g);
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
+        }
+        ws = wait_stream(ctx);  // the temporaries above are freed on return
+        if (ws != PA_OK) return ws;
+    }
+    fill_batch_view(B, view<F>(B), desc);
+    return wait_stream(ctx);
+}
+
+template <typename F, int NS>
+void launch_pose(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, const F* rho2, const int32_t* reach0,
+                 cudaStream_t st) {
+    const pa::DevBatch<F>& d = cview<F>(B);
+    unsigned grid = unsigned((ca.n_act + 255) / 256);
+    pa::k_pose<F, NS><<<grid, 256, 0, st>>>(d, ca, w, rho2, reach0);
+}
+
+template <int NS>
+cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms, cudaStream_t st) {
+    if (B->precision == PA_PRECISION_F32) {
+        size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
+        if (dyn > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+            if (e != cudaSuccess) return e;
+        }
+        pa::k_energy32<NS><<<num_sms * 4, PA_TILE32, dyn, st>>>(B->d32, ca, w);
+    } else {
+        pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
+    }
+    return cudaGetLastError();
+}
+
+#define PA_DISPATCH_NS(N, EXPR)                              \
+    switch (N) {                                             \
+        case 1: { constexpr int NSV = 1; EXPR; } break;      \
+        case 2: { constexpr int NSV = 2; EXPR; } break;      \
+        case 3: { constexpr int NSV = 3; EXPR; } break;      \
+        case 4: { constexpr int NSV = 4; EXPR; } break;      \
+        case 5: { constexpr int NSV = 5; EXPR; } break;      \
+        case 6: { constexpr int NSV = 6; EXPR; } break;      \
+        case 7: { constexpr int NSV = 7; EXPR; } break;      \
+        default: { constexpr int NSV = 8; EXPR; } break;     \
+    }
+
+}  // namespace
+
+extern "C" {
+
+const char* pa_version(void) { return "pureadsorb-b200 0.1.0"; }
+
+pa_status pa_context_create(int32_t device, pa_context** out) {
+    if (!out) return PA_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return PA_ERR_CUDA;
+    if (device < 0 || device >= n) return PA_ERR_ARG;
+    pa_context* ctx = new pa_context();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
+    ctx->stream = ctx->own;
+    *out = ctx;
+    return PA_OK;
+}
+
+pa_status pa_context_destroy(pa_context* ctx) {
+    if (!ctx) return PA_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return PA_OK;
+}
+
+pa_status pa_context_set_stream(pa_context* ctx, void* stream) {
+    if (!ctx) return PA_ERR_ARG;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+    return PA_OK;
+}
+
+const char* pa_last_error(const pa_context* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+pa_status pa_context_set_timing(pa_context* ctx, int32_t enable) {
+    if (!ctx) return PA_ERR_ARG;
+    ctx->timing = enable != 0;
+    for (int c = 0; c < NCLASS; ++c) { ctx->ms[c] = 0; ctx->launches[c] = 0; }
+    return PA_OK;
+}
+
+pa_status pa_context_kernel_times(pa_context* ctx, double* ms, int64_t* launches) {
+    if (!ctx || !ms || !launches) return PA_ERR_ARG;
+    for (int c = 0; c < NCLASS; ++c) { ms[c] = ctx->ms[c]; launches[c] = ctx->launches[c]; }
+    return PA_OK;
+}
+
+pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t precision, pa_batch** out) {
+    if (!ctx || !desc || !out) return fail(ctx, PA_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (precision != PA_PRECISION_F32 && precision != PA_PRECISION_F64) return fail(ctx, PA_ERR_ARG, "precision must be 32 or 64");
+    if (desc->nsys < 1 || desc->nfw < 1 || desc->ntypes < 1 || desc->nguest < 1)
+        return fail(ctx, PA_ERR_ARG, "batch needs nsys, nfw, ntypes, nguest >= 1");
+    if (desc->nguest > PA_MAX_GUEST_SITES) return fail(ctx, PA_ERR_ARG, "guest has more than PA_MAX_GUEST_SITES sites");
+    if (!desc->atom_offsets || !desc->k_offsets || !desc->cellgrid_offsets || !desc->framework_of || !desc->cells ||
+        !desc->invcells || !desc->sigma || !desc->epsilon || !desc->guest_types || !desc->guest_sites ||
+        !desc->guest_charges || !desc->alphas || !desc->constant_offset || !desc->ncells)
+        return fail(ctx, PA_ERR_ARG, "batch descriptor has a null array");
+    const int nfw = desc->nfw;
+    if (desc->atom_offsets[0] != 0 || desc->k_offsets[0] != 0 || desc->cellgrid_offsets[0] != 0)
+        return fail(ctx, PA_ERR_ARG, "offsets must start at 0");
+    for (int f = 0; f < nfw; ++f) {
+        if (desc->atom_offsets[f + 1] < desc->atom_offsets[f] || desc->k_offsets[f + 1] < desc->k_offsets[f] ||
+            desc->cellgrid_offsets[f + 1] <= desc->cellgrid_offsets[f])
+            return fail(ctx, PA_ERR_ARG, "offsets must be non-decreasing");
+        int64_t ncell = int64_t(desc->ncells[3 * f]) * desc->ncells[3 * f + 1] * desc->ncells[3 * f + 2];
+        if (desc->cellgrid_offsets[f + 1] - desc->cellgrid_offsets[f] != ncell + 1)
+            return fail(ctx, PA_ERR_ARG, "framework " + std::to_string(f + 1) + ": cellgrid_offsets does not match ncells");
+        if (desc->cell_offsets[desc->cellgrid_offsets[f + 1] - 1] != desc->atom_offsets[f + 1] - desc->atom_offsets[f])
+            return fail(ctx, PA_ERR_ARG, "framework " + std::to_string(f + 1) + ": last cell_offsets entry must equal its atom count");
+    }
+    const int64_t na = desc->atom_offsets[nfw], nk = desc->k_offsets[nfw];
+    if (na > 0 && (!desc->positions || !desc->types || !desc->charges)) return fail(ctx, PA_ERR_ARG, "batch has atoms but null atom arrays");
+    if (nk > 0 && (!desc->ks || !desc->kprefactor || !desc->Shost)) return fail(ctx, PA_ERR_ARG, "batch has k-vectors but null k arrays");
+    for (int64_t j = 0; j < na; ++j)
+        if (desc->types[j] < 1 || desc->types[j] > desc->ntypes) return fail(ctx, PA_ERR_ARG, "atom type out of range");
+    for (int s = 0; s < desc->nsys; ++s)
+        if (desc->framework_of[s] < 1 || desc->framework_of[s] > nfw) return fail(ctx, PA_ERR_ARG, "framework_of out of range");
+    for (int a = 0; a < desc->nguest; ++a)
+        if (desc->guest_types[a] < 1 || desc->guest_types[a] > desc->ntypes) return fail(ctx, PA_ERR_ARG, "guest type out of range");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    pa_batch* B = new pa_batch();
+    B->ctx = ctx; B->precision = precision;
+    B->nsys = desc->nsys; B->nfw = nfw; B->ntypes = desc->ntypes; B->nguest = desc->nguest;
+    B->natoms = na; B->nk = nk;
+    B->framework_of.assign(desc->framework_of, desc->framework_of + desc->nsys);
+    B->atom_offsets.assign(desc->atom_offsets, desc->atom_offsets + nfw + 1);
+    B->k_offsets.assign(desc->k_offsets, desc->k_offsets + nfw + 1);
+    pa_status st = precision == PA_PRECISION_F32 ? upload_impl<float>(ctx, desc, B) : upload_impl<double>(ctx, desc, B);
+    if (ctx->timing) Timer::collect(ctx);
+    if (st != PA_OK) { delete B; return st; }
+    *out = B;
+    return PA_OK;
+}
+
+pa_status pa_batch_free(pa_batch* batch) {
+    if (!batch) return PA_ERR_ARG;
+    cudaSetDevice(batch->ctx->device);
+    cudaStreamSynchronize(batch->ctx->stream);
+    delete batch;
+    return PA_OK;
+}
+
+pa_status pa_batch_info(const pa_batch* batch, int64_t* list_entries, int64_t* nbins) {
+    if (!batch) return PA_ERR_ARG;
+    if (list_entries) *list_entries = batch->list_entries;
+    if (nbins) *nbins = batch->nbins;
+    return PA_OK;
+}
+
+pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args, pa_block_sums* sums,
+                   pa_insertion_out* per) {
+    if (!ctx || !B || !args || !sums) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
+    if (!sums->lse_max || !sums->sum_w || !sums->sum_uw || !sums->count) return fail(ctx, PA_ERR_ARG, "null block-sum array");
+    const int64_t ninsert = args->ninsert, nblocks = args->nblocks, run = args->run;
+    if (ninsert < 1) return fail(ctx, PA_ERR_ARG, "ninsert must be >= 1");
+    if (nblocks < 1) return fail(ctx, PA_ERR_ARG, "nblocks must be >= 1");
+    if (run < 1) return fail(ctx, PA_ERR_ARG, "run must be >= 1");
+    if (!(std::isfinite(args->kT) && args->kT != 0)) return fail(ctx, PA_ERR_ARG, "kT must be finite and nonzero");
+    if (args->reject && (!args->rho2 || !args->reach0)) return fail(ctx, PA_ERR_ARG, "reject needs rho2 and reach0");
+    const int nsys = B->nsys, N = B->nguest, nt = B->ntypes;
+    std::vector<int64_t> ns = system_counts(ninsert, nsys, run);
+    for (int s = 0; s < nsys; ++s)
+        if (ns[s] < nblocks)
+            return fail(ctx, PA_ERR_ARG, "system " + std::to_string(s + 1) + " gets " + std::to_string(ns[s]) +
+                                             " samples, fewer than nblocks");
+    std::vector<int64_t> off(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) off[s + 1] = off[s] + ns[s];
+    std::vector<Seg> segs = segments(ns, off, nblocks);
+    const int64_t nseg_all = int64_t(segs.size());
+    int64_t sb = std::max<int64_t>(0, args->segment_begin), se = args->segment_end <= 0 ? nseg_all : std::min(args->segment_end, nseg_all);
+    for (int64_t q = 0; q < nsys * nblocks; ++q) {
+        sums->lse_max[q] = -INFINITY; sums->sum_w[q] = 0; sums->sum_uw[q] = 0; sums->count[q] = 0;
+    }
+    if (sb >= se) return PA_OK;
+    const int64_t i_lo = segs[sb].i0, i_hi = segs[se - 1].i1, n_act = i_hi - i_lo;
+    if (n_act > INT32_MAX) return fail(ctx, PA_ERR_ARG, "one call processes at most 2^31-1 insertions");
+    const int64_t nseg = se - sb;
+    std::vector<int64_t> seg_rng(2 * nseg);
+    for (int64_t q = 0; q < nseg; ++q) { seg_rng[2 * q] = segs[sb + q].i0 - i_lo; seg_rng[2 * q + 1] = segs[sb + q].i1 - i_lo; }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    const bool f32 = B->precision == PA_PRECISION_F32;
+    // workspace
+    PA_CUDA(ctx, ctx->pose_a.ensure((f32 ? sizeof(float4) : sizeof(double4)) * n_act));
+    PA_CUDA(ctx, ctx->pose_b.ensure((f32 ? sizeof(float4) : sizeof(double4)) * n_act));
+    PA_CUDA(ctx, ctx->bin_of.ensure(sizeof(int32_t) * n_act));
+    PA_CUDA(ctx, ctx->slot.ensure(sizeof(int32_t) * n_act));
+    PA_CUDA(ctx, ctx->sorted.ensure(sizeof(int32_t) * n_act));
+    PA_CUDA(ctx, ctx->dU.ensure(sizeof(double) * n_act));
+    PA_CUDA(ctx, ctx->bin_count.ensure(sizeof(int32_t) * (B->nbins + 1)));
+    PA_CUDA(ctx, ctx->bin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+    PA_CUDA(ctx, ctx->tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+    PA_CUDA(ctx, ctx->counters.ensure(sizeof(int32_t) * 8));
+    PA_CUDA(ctx, ctx->seg_out.ensure(sizeof(double) * 3 * nseg));
+    PA_CUDA(ctx, upload(ctx->seg_rng, seg_rng, st));
+    PA_CUDA(ctx, upload(ctx->sys_off, off, st));
+    if (args->reject) {
+        std::vector<int32_t> r0(args->reach0, args->reach0 + 3 * nsys);
+        PA_CUDA(ctx, upload(ctx->reach0, r0, st));
+        const int64_t nr = int64_t(nsys) * N * nt;
+        if (f32) { std::vector<float> r2(nr); for (int64_t q = 0; q < nr; ++q) r2[q] = float(args->rho2[q]); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
+        else { std::vector<double> r2(args->rho2, args->rho2 + nr); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
+    }
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (B->nbins + 1), st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 8, st));
+    pa::Work w{};
+    if (f32) { w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>(); }
+    else { w.pose64a = ctx->pose_a.as<double4>(); w.pose64b = ctx->pose_b.as<double4>(); }
+    w.bin_of = ctx->bin_of.as<int32_t>(); w.slot = ctx->slot.as<int32_t>(); w.sorted = ctx->sorted.as<int32_t>();
+    w.dU = ctx->dU.as<double>(); w.bin_count = ctx->bin_count.as<int32_t>(); w.bin_start = ctx->bin_start.as<int32_t>();
+    w.tile_start = ctx->tile_start.as<int32_t>(); w.counters = ctx->counters.as<int32_t>();
+    w.seg_out = ctx->seg_out.as<double>(); w.seg_rng = ctx->seg_rng.as<int64_t>();
+    pa::CallArgs ca{};
+    ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
+    ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
+    {
+        Timer tm(ctx, 0);
+        if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, ctx->rho2.as<float>(), ctx->reach0.as<int32_t>(), st))); }
+        else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, ctx->rho2.as<double>(), ctx->reach0.as<int32_t>(), st))); }
+        tm.stop(1);
+        PA_CUDA(ctx, cudaGetLastError());
+    }
+    {
+        Timer tm(ctx, 1);
+        pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, f32 ? PA_TILE32 : PA_TILE64);
+        pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
+        tm.stop(2);
+        PA_CUDA(ctx, cudaGetLastError());
+    }
+    {
+        Timer tm(ctx, 2);
+        cudaError_t e = cudaSuccess;
+        PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, st)));
+        tm.stop(1);
+        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+    }
+    {
+        Timer tm(ctx, 3);
+        pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT);
+        tm.stop(1);
+        PA_CUDA(ctx, cudaGetLastError());
+    }
+    std::vector<double> seg_out(3 * nseg);
+    int32_t counters[8];
+    PA_CUDA(ctx, cudaMemcpyAsync(seg_out.data(), ctx->seg_out.p, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(counters, ctx->counters.p, sizeof(counters), cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> bin_of;
+    std::vector<char> pose_a, pose_b;
+    if (per && per->dU)
+        PA_CUDA(ctx, cudaMemcpyAsync(per->dU + i_lo, ctx->dU.p, sizeof(double) * n_act, cudaMemcpyDeviceToHost, st));
+    if (per && per->flags) {
+        bin_of.resize(n_act);
+        PA_CUDA(ctx, cudaMemcpyAsync(bin_of.data(), ctx->bin_of.p, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st));
+    }
+    if (per && per->poses) {
+        size_t vb = (f32 ? sizeof(float4) : sizeof(double4)) * n_act;
+        pose_a.resize(vb); pose_b.resize(vb);
+        PA_CUDA(ctx, cudaMemcpyAsync(pose_a.data(), ctx->pose_a.p, vb, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(pose_b.data(), ctx->pose_b.p, vb, cudaMemcpyDeviceToHost, st));
+    }
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    if (ctx->timing) Timer::collect(ctx);
+    if (counters[2] != 0) return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
+    if (per && per->flags)
+        for (int64_t t = 0; t < n_act; ++t) per->flags[i_lo + t] = bin_of[t] < 0 ? 1 : 0;
+    if (per && per->poses)
+        for (int64_t t = 0; t < n_act; ++t) {
+            double* o = per->poses + 7 * (i_lo + t);
+            if (f32) {
+                const float4 a = reinterpret_cast<const float4*>(pose_a.data())[t], b = reinterpret_cast<const float4*>(pose_b.data())[t];
+                o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = b.x; o[4] = b.y; o[5] = b.z; o[6] = b.w;
+            } else {
+                const double4 a = reinterpret_cast<const double4*>(pose_a.data())[t], b = reinterpret_cast<const double4*>(pose_b.data())[t];
+                o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = b.x; o[4] = b.y; o[5] = b.z; o[6] = b.w;
+            }
+        }
+    // block sums from the processed segments, in segment order
+    if (sums->segments)
+        for (int64_t q = 0; q < nseg; ++q)
+            for (int r = 0; r < 3; ++r) sums->segments[3 * (sb + q) + r] = seg_out[3 * q + r];
+    for (int64_t q = 0; q < nseg; ++q) {
+        const Seg& g = segs[sb + q];
+        combine_segment(sums, g.s * nblocks + g.b, g.i1 - g.i0, seg_out.data() + 3 * q);
+    }
+    return PA_OK;
+}
+
+pa_status pa_segment_count(int64_t ninsert, int32_t nsys, int32_t run, int32_t nblocks, int64_t* nseg) {
+    if (!nseg || ninsert < 1 || nsys < 1 || run < 1 || nblocks < 1) return PA_ERR_ARG;
+    std::vector<int64_t> ns = system_counts(ninsert, nsys, run);
+    for (int s = 0; s < nsys; ++s) if (ns[s] < nblocks) return PA_ERR_ARG;
+    std::vector<int64_t> off(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) off[s + 1] = off[s] + ns[s];
+    *nseg = int64_t(segments(ns, off, nblocks).size());
+    return PA_OK;
+}
+
+pa_status pa_combine_segments(int64_t ninsert, int32_t nsys, int32_t run, int32_t nblocks, const double* segs_in,
+                              pa_block_sums* sums) {
+    if (!segs_in || !sums || !sums->lse_max || !sums->sum_w || !sums->sum_uw || !sums->count) return PA_ERR_ARG;
+    if (ninsert < 1 || nsys < 1 || run < 1 || nblocks < 1) return PA_ERR_ARG;
+    std::vector<int64_t> ns = system_counts(ninsert, nsys, run);
+    for (int s = 0; s < nsys; ++s) if (ns[s] < nblocks) return PA_ERR_ARG;
+    std::vector<int64_t> off(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) off[s + 1] = off[s] + ns[s];
+    std::vector<Seg> segs = segments(ns, off, nblocks);
+    for (int64_t q = 0; q < int64_t(nsys) * nblocks; ++q) {
+        sums->lse_max[q] = -INFINITY; sums->sum_w[q] = 0; sums->sum_uw[q] = 0; sums->count[q] = 0;
+    }
+    for (size_t q = 0; q < segs.size(); ++q)
+        combine_segment(sums, segs[q].s * nblocks + segs[q].b, segs[q].i1 - segs[q].i0, segs_in + 3 * q);
+    return PA_OK;
+}
+
+pa_status pa_pose_host(int32_t precision, uint64_t seed, uint64_t s, uint64_t k, double* rpos, double* quat) {
+    if (!rpos || !quat) return PA_ERR_ARG;
+    if (precision == PA_PRECISION_F32) {
+        float r[3], q[4];
+        pa::draw_pose<float>(seed, s, k, r, q);
+        for (int i = 0; i < 3; ++i) rpos[i] = r[i];
+        for (int i = 0; i < 4; ++i) quat[i] = q[i];
+        return PA_OK;
+    }
+    if (precision != PA_PRECISION_F64) return PA_ERR_ARG;
+    pa::draw_pose<double>(seed, s, k, rpos, quat);
+    return PA_OK;
+}
+
+pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, const double* positions,
+                              const double* charges, int64_t natoms, double* S) {
+    if (!ctx || (nk > 0 && (!ks || !S)) || (natoms > 0 && (!positions || !charges))) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (nk == 0) return PA_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    DevMem dk, dp, dq, dS;
+    std::vector<double> vk(ks, ks + 3 * nk), vp(positions, positions + 3 * natoms), vq(charges, charges + natoms);
+    PA_CUDA(ctx, upload(dk, vk, st));
+    PA_CUDA(ctx, upload(dp, vp, st));
+    PA_CUDA(ctx, upload(dq, vq, st));
+    PA_CUDA(ctx, dS.ensure(sizeof(double) * 2 * nk));
+    pa::k_structure_factor<<<unsigned((nk + 255) / 256), 256, 0, st>>>(dk.as<double>(), nk, dp.as<double>(), dq.as<double>(), natoms, dS.as<double>());
+    PA_CUDA(ctx, cudaGetLastError());
+    PA_CUDA(ctx, cudaMemcpyAsync(S, dS.p, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost, st));
+    return wait_stream(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,772 @@
+// Device kernels of the B200 Widom path.
+//
+// Pipeline of one widom call (pa_widom in pa_capi.cu):
+//   k_pose      one thread per insertion: counter-based pose, phase-0 hard-core scan over the
+//               cell list (strict arithmetic, bit-identical to the oracle), and for survivors a
+//               spatial bin plus a slot in it (src/widom.jl:99-151, 399-415);
+//   k_scan      one CTA: exclusive scans of the bin counts and of the per-bin tile counts;
+//   k_scatter   survivors into bin-sorted order;
+//   k_energy32  persistent CTAs over (bin, tile) work items: the bin's imaged neighbour list is
+//               streamed into shared memory by bulk copies (cp.async.bulk + mbarrier, double
+//               buffered), one insertion per thread, FP32 pair arithmetic with compensated sums,
+//               reciprocal term against FP64-built per-bin phase factors (src/energy.jl:42-82);
+//   k_energy64  the plain FP64 form of the reference algorithm (linear loop over every atom,
+//               one minimum image per atom), tiles per framework;
+//   k_segsum    per PA_SEGMENT-insertion segment: max, then Σ exp(x - max) and Σ ΔU exp(x - max),
+//               x = -ΔU/kT, with a fixed reduction tree (src/widom.jl:80-84, 430-438).
+#pragma once
+#include <cuda_runtime.h>
+#include "pa_common.cuh"
+
+#define PA_SEGMENT_SIZE 2048
+
+namespace pa {
+
+template <typename F> struct Vec4;
+template <> struct Vec4<float> { typedef float4 T; };
+template <> struct Vec4<double> { typedef double4 T; };
+
+// Device view of an uploaded batch. Index conventions are 0-based on the device.
+template <typename F>
+struct DevBatch {
+    int32_t nsys, nfw, ntypes, nguest, has_charge, nbins;
+    F rl2, re2;                                   // LJ and Ewald cutoffs squared
+    const int32_t* framework_of;                  // nsys
+    const F* cells;                               // 9*nfw column-major
+    const F* invcells;                            // 9*nfw
+    const double* alphas;                         // nfw
+    const double* const_offset;                   // nfw
+    const int32_t* atom_offsets;                  // nfw+1
+    const typename Vec4<F>::T* atoms;             // cell-sorted x, y, z, q
+    const int32_t* types;                         // 0-based compact
+    const int32_t* ncells;                        // 3*nfw
+    const int32_t* cell_offsets;
+    const int32_t* cellgrid_offsets;              // nfw+1
+    const int32_t* k_offsets;                     // nfw+1
+    const double* kvec;                           // 3*nk Cartesian (FP64 path)
+    const float* kcoef;                           // 3*nk integer coefficients as float (FP32 path)
+    const double* kS2;                            // 2*nk: 2*kpref*S_re, 2*kpref*S_im (FP64)
+    const F* sig2;                                // nguest*ntypes: sigma^2 of (site, host type)
+    const F* eps4;                                // nguest*ntypes: 4 eps
+    F gsite[3 * PA_MAX_SITES_DEV];
+    F gq[PA_MAX_SITES_DEV];
+    // spatial bins (FP32 path: per-framework fractional grids; FP64 path: one bin per framework)
+    const int32_t* bin_dims;                      // 3*nfw
+    const int32_t* bin_base;                      // nfw+1
+    const int32_t* bin_fw;                        // nbins
+    const int32_t* list_offsets;                  // nbins+1, multiples of PA_LIST_PAD
+    const float4* list_xyzq;                      // imaged position relative to the bin centre, charge
+    const int32_t* list_type;                     // 0-based type (padding entries: type 0, far away)
+};
+
+// Per-call arguments shared by the kernels.
+struct CallArgs {
+    int64_t i_lo, n_act;        // processed insertions: global indices [i_lo, i_lo + n_act)
+    const int64_t* sys_off;     // nsys+1 insertion offsets (system-major)
+    uint64_t seed;
+    int32_t reject;
+    double kT;
+};
+
+// Per-call device workspace.
+struct Work {
+    float4* pose_a;    // FP32 path: rpos.xyz; FP64 path uses pose64
+    float4* pose_b;    // quaternion
+    double4* pose64a;  // FP64 path rpos (xyz)
+    double4* pose64b;  // FP64 path quaternion
+    int32_t* bin_of;   // n_act: bin of a survivor, -1 if rejected
+    int32_t* slot;     // n_act
+    int32_t* sorted;   // n_act: local insertion index in bin order
+    double* dU;        // n_act: ΔU (+inf if rejected)
+    int32_t* bin_count;   // nbins
+    int32_t* bin_start;   // nbins+1
+    int32_t* tile_start;  // nbins+1
+    int32_t* counters;    // [0] tile cursor, [1] total tiles, [2] error code, [3] survivors
+    double* seg_out;      // 3 per segment: max, Σ w, Σ ΔU w
+    const int64_t* seg_rng;  // 2 per segment: local [begin, end)
+};
+
+// ---------------------------------------------------------------------------------------------
+// Small helpers
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int32_t find_system(const int64_t* sys_off, int32_t nsys, int64_t i) {
+    int32_t lo = 0, hi = nsys;  // sys_off[lo] <= i < sys_off[hi]
+    while (hi - lo > 1) {
+        int32_t mid = (lo + hi) >> 1;
+        if (sys_off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ int32_t find_bin(const int32_t* start, int32_t n, int32_t t) {
+    int32_t lo = 0, hi = n;  // largest b with start[b] <= t
+    while (hi - lo > 1) {
+        int32_t mid = (lo + hi) >> 1;
+        if (start[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ void kahan_add(float& sum, float& c, float x) {
+    float y = __fsub_rn(x, c);
+    float t = __fadd_rn(sum, y);
+    c = __fsub_rn(__fsub_rn(t, sum), y);
+    sum = t;
+}
+
+// Phase 0 for one pose: any guest site closer than sqrt(rho2[s, a, type]) to a host atom, over
+// the per-site cell stencil (src/widom.jl:99-151). Strict arithmetic (bit-identical to the
+// oracle's hardcore_flag).
+template <typename F, int NS>
+__device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const F* rp, const F* qt,
+                              const F* rho2, const int32_t* reach0) {
+    typedef St<F> S;
+    const F* A = b.cells + 9 * fw;
+    const F* iA = b.invcells + 9 * fw;
+    F Ael[9], iAel[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) { Ael[r] = A[r]; iAel[r] = iA[r]; }
+    const int32_t a0 = b.atom_offsets[fw];
+    const int32_t* coff = b.cell_offsets + b.cellgrid_offsets[fw];
+    const int32_t n1 = b.ncells[3 * fw], n2 = b.ncells[3 * fw + 1], n3 = b.ncells[3 * fw + 2];
+    const int32_t m1 = reach0[3 * s], m2 = reach0[3 * s + 1], m3 = reach0[3 * s + 2];
+    const int32_t nt = b.ntypes;
+    F pos[3];
+    matvec_s(Ael, rp, pos);
+    const F* r2row = rho2 + int64_t(s) * NS * nt;
+#pragma unroll 1
+    for (int a = 0; a < NS; ++a) {
+        F g[3];
+        rotate_s(qt, b.gsite + 3 * a, g);
+        F sp[3] = {S::add(pos[0], g[0]), S::add(pos[1], g[1]), S::add(pos[2], g[2])};
+        F f[3];
+        matvec_s(iAel, sp, f);
+        int32_t h1 = home_cell_s(wrap_frac_s(f[0]), n1);
+        int32_t h2 = home_cell_s(wrap_frac_s(f[1]), n2);
+        int32_t h3 = home_cell_s(wrap_frac_s(f[2]), n3);
+        int32_t st1, c1, st2, c2, st3, c3;
+        stencil_start_count(h1, m1, n1, &st1, &c1);
+        stencil_start_count(h2, m2, n2, &st2, &c2);
+        stencil_start_count(h3, m3, n3, &st3, &c3);
+        const F* r2a = r2row + a * nt;
+        for (int32_t t3 = 0; t3 < c3; ++t3) {
+            int32_t z = wrap_cell(st3 + t3, n3);
+            for (int32_t t2 = 0; t2 < c2; ++t2) {
+                int32_t y = wrap_cell(st2 + t2, n2);
+                for (int32_t t1 = 0; t1 < c1; ++t1) {
+                    int32_t x = wrap_cell(st1 + t1, n1);
+                    int32_t c = x + n1 * (y + n2 * z);
+                    int32_t j1 = a0 + coff[c + 1];
+                    for (int32_t j = a0 + coff[c]; j < j1; ++j) {
+                        typename Vec4<F>::T at = b.atoms[j];
+                        F D[3] = {S::sub(sp[0], at.x), S::sub(sp[1], at.y), S::sub(sp[2], at.z)};
+                        minimum_image_s(Ael, iAel, D);
+                        F r2 = dot3s(D[0], D[1], D[2], D[0], D[1], D[2]);
+                        if (r2 < r2a[b.types[j]]) return true;
+                    }
+                }
+            }
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_pose: pose, phase 0, bin slot
+// ---------------------------------------------------------------------------------------------
+template <typename F, int NS>
+__global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w, const F* rho2, const int32_t* reach0) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= ca.n_act) return;
+    const int64_t i = ca.i_lo + t;
+    const int32_t s = find_system(ca.sys_off, b.nsys, i);
+    const int64_t k = i - ca.sys_off[s] + 1;
+    const int32_t fw = b.framework_of[s];
+    F rp[3], qt[4];
+    draw_pose<F>(ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    if (sizeof(F) == 4) {
+        w.pose_a[t] = make_float4(float(rp[0]), float(rp[1]), float(rp[2]), 0.0f);
+        w.pose_b[t] = make_float4(float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3]));
+    } else {
+        w.pose64a[t] = make_double4(double(rp[0]), double(rp[1]), double(rp[2]), 0.0);
+        w.pose64b[t] = make_double4(double(qt[0]), double(qt[1]), double(qt[2]), double(qt[3]));
+    }
+    if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0)) {
+        w.bin_of[t] = -1;
+        w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+        return;
+    }
+    const int32_t* nb = b.bin_dims + 3 * fw;
+    int32_t bx = min(int32_t(float(rp[0]) * float(nb[0])), nb[0] - 1);
+    int32_t by = min(int32_t(float(rp[1]) * float(nb[1])), nb[1] - 1);
+    int32_t bz = min(int32_t(float(rp[2]) * float(nb[2])), nb[2] - 1);
+    int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
+    w.bin_of[t] = bin;
+    w.slot[t] = atomicAdd(&w.bin_count[bin], 1);
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_scan: one CTA of 1024 threads; exclusive scans of bin counts and of tile counts
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* s_warp, int32_t* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int32_t z = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        if (lane < nw) s_warp[lane] = z;  // inclusive warp prefix
+    }
+    __syncthreads();
+    int32_t warp_excl = wid == 0 ? 0 : s_warp[wid - 1];
+    *total = s_warp[nw - 1];
+    __syncthreads();
+    return warp_excl + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan(Work w, int32_t nbins, int32_t tile) {
+    __shared__ int32_t s_warp[32];
+    int32_t carry_b = 0, carry_t = 0;
+    for (int32_t base = 0; base < nbins; base += blockDim.x) {
+        int32_t b = base + threadIdx.x;
+        int32_t c = b < nbins ? w.bin_count[b] : 0;
+        int32_t nt = (c + tile - 1) / tile;
+        int32_t tb, tt;
+        int32_t eb = block_excl_scan(c, s_warp, &tb);
+        int32_t et = block_excl_scan(nt, s_warp, &tt);
+        if (b < nbins) { w.bin_start[b] = carry_b + eb; w.tile_start[b] = carry_t + et; }
+        carry_b += tb; carry_t += tt;
+    }
+    if (threadIdx.x == 0) {
+        w.bin_start[nbins] = carry_b;
+        w.tile_start[nbins] = carry_t;
+        w.counters[1] = carry_t;
+        w.counters[3] = carry_b;
+    }
+}
+
+__global__ void k_scatter(Work w, int64_t n_act) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n_act) return;
+    int32_t bin = w.bin_of[t];
+    if (bin >= 0) w.sorted[w.bin_start[bin] + w.slot[t]] = int32_t(t);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Bulk-copy pipeline primitives (cp.async.bulk, mbarrier), with bounded waits.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for phase `parity` of `bar`; gives up after PA_WAIT_LIMIT polls and returns false.
+#define PA_WAIT_LIMIT (1 << 26)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < PA_WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// FP32 screened Coulomb: erfc(z)/r with z = alpha r, r = sqrt(r2). erfc(z) = exp(-z^2) P(t),
+// t = 2/(2+z), P a degree-9 fit (gen_coeffs.py), ~2e-7 relative on [0, 4].
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
+    float ri = rsqrtf(r2);
+    ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);  // one Newton step
+    float r = r2 * ri;
+    float z = alpha * r;
+    float d = fmaf(0.5f, z, 1.0f);
+    float t = __frcp_rn(d);
+    const float c[PA_NERFC32] = PA_ERFC32_INIT;
+    float p = c[PA_NERFC32 - 1];
+#pragma unroll
+    for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, t, c[k]);
+    float e = __expf(-z * z);
+    return p * e * ri;
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_energy32: persistent CTAs over (bin, tile) items; one insertion per thread.
+// ---------------------------------------------------------------------------------------------
+#define PA_TILE32 128
+#define PA_CHUNK32 256
+#define PA_KCHUNK 256
+
+template <int NS>
+__global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
+    __shared__ __align__(128) float4 s_xyzq[2][PA_CHUNK32];
+    __shared__ __align__(128) int32_t s_type[2][PA_CHUNK32];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ float2 s_B[PA_KCHUNK];
+    __shared__ float s_kc[3 * PA_KCHUNK];
+    __shared__ int32_t s_item[4];
+    extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
+    const int tid = threadIdx.x;
+    const int nt = b.ntypes;
+    for (int x = tid; x < NS * nt; x += blockDim.x) { s_lj[x] = b.sig2[x]; s_lj[NS * nt + x] = b.eps4[x]; }
+    if (tid == 0) { mbar_init(&s_bar[0], 1); mbar_init(&s_bar[1], 1); mbar_fence_init(); }
+    __syncthreads();
+    const float* s_sig2 = s_lj;
+    const float* s_eps4 = s_lj + NS * nt;
+    uint32_t gchunk = 0;  // chunks consumed by this CTA so far (selects stage and parity)
+    const int32_t total_tiles = w.counters[1];
+    for (;;) {
+        if (tid == 0) {
+            int32_t t = atomicAdd(&w.counters[0], 1);
+            s_item[0] = t;
+            if (t < total_tiles) {
+                int32_t bin = find_bin(w.tile_start, b.nbins, t);
+                int32_t j0 = (t - w.tile_start[bin]) * PA_TILE32;
+                int32_t lo = w.bin_start[bin] + j0;
+                int32_t hi = min(lo + PA_TILE32, w.bin_start[bin + 1]);
+                s_item[1] = bin; s_item[2] = lo; s_item[3] = hi;
+            }
+        }
+        __syncthreads();
+        const int32_t t = s_item[0];
+        if (t >= total_tiles) break;
+        const int32_t bin = s_item[1], lo = s_item[2], hi = s_item[3];
+        __syncthreads();  // s_item may be overwritten at the next item
+        const int32_t fw = b.bin_fw[bin];
+        const int32_t l0 = b.list_offsets[bin], l1 = b.list_offsets[bin + 1];
+        const int32_t nch = (l1 - l0 + PA_CHUNK32 - 1) / PA_CHUNK32;
+        // prologue: first two chunks in flight
+        if (tid == 0) {
+            for (int c = 0; c < 2 && c < nch; ++c) {
+                uint32_t st = (gchunk + c) & 1;
+                int32_t e0 = l0 + c * PA_CHUNK32, n = min(PA_CHUNK32, l1 - e0);
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&s_bar[st], uint32_t(n) * 20u);
+                bulk_g2s(s_xyzq[st], b.list_xyzq + e0, uint32_t(n) * 16u, &s_bar[st]);
+                bulk_g2s(s_type[st], b.list_type + e0, uint32_t(n) * 4u, &s_bar[st]);
+            }
+        }
+        // this thread's insertion
+        const bool active = lo + tid < hi;
+        const int32_t li = active ? w.sorted[lo + tid] : 0;
+        const int32_t* nb = b.bin_dims + 3 * fw;
+        const int32_t lb = bin - b.bin_base[fw];
+        const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
+        const float cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
+        const float cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
+        const float cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
+        float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
+        float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
+        const float* A = b.cells + 9 * fw;
+        const float* iA = b.invcells + 9 * fw;
+        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
+        float px[NS], py[NS], pz[NS], dfr[3 * NS];
+        {
+            const float q[4] = {pq.x, pq.y, pq.z, pq.w};
+            float gsb[3 * NS];
+#pragma unroll
+            for (int x = 0; x < 3 * NS; ++x) gsb[x] = b.gsite[x];
+            const float c0 = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0));
+            const float c1 = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0));
+            const float c2 = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0));
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                float g[3];
+                rotate_s(q, gsb + 3 * s, g);
+                px[s] = c0 + g[0]; py[s] = c1 + g[1]; pz[s] = c2 + g[2];
+                // fractional offset of the site from the bin centre, for the reciprocal term
+                dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
+                dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
+                dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
+            }
+        }
+        float gqs[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) gqs[s] = b.gq[s];
+        const float rl2 = b.rl2, re2 = b.re2, alpha = float(b.alphas[fw]);
+        const bool charged = b.has_charge != 0;
+        float elj = 0.f, clj = 0.f, esr = 0.f, csr = 0.f;
+        // tmo_at: chunk whose bulk copy did not arrive in time (-1: none). After a timeout no
+        // further copies are issued and only the chunk already in flight is still waited for.
+        int32_t tmo_at = -1;
+        for (int32_t c = 0; c < nch; ++c) {
+            const uint32_t g = gchunk + c, st = g & 1, par = (g >> 1) & 1;
+            const bool issued = tmo_at < 0 || c == tmo_at + 1;
+            if (!issued) break;
+            const bool late = !mbar_wait_bounded(&s_bar[st], par);
+            const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
+            if (tmo_at < 0 && !late) {
+#pragma unroll 2
+                for (int32_t j = 0; j < n; ++j) {
+                    const float4 at = s_xyzq[st][j];
+                    const int32_t ty = s_type[st][j];
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (r2 < rl2) {
+                            const float inv = __frcp_rn(r2);
+                            const float x = s_sig2[s * nt + ty] * inv;
+                            const float x3 = x * x * x;
+                            kahan_add(elj, clj, s_eps4[s * nt + ty] * (x3 * x3 - x3));
+                        }
+                        if (charged && r2 < re2) kahan_add(esr, csr, gqs[s] * at.w * erfc_over_r(r2, alpha));
+                    }
+                }
+            }
+            // every thread is done with stage st; a late copy anywhere stops the pipeline
+            if (__syncthreads_or(late) && tmo_at < 0) tmo_at = c;
+            if (tid == 0 && tmo_at < 0 && c + 2 < nch) {
+                int32_t e0 = l0 + (c + 2) * PA_CHUNK32, nn = min(PA_CHUNK32, l1 - e0);
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&s_bar[st], uint32_t(nn) * 20u);
+                bulk_g2s(s_xyzq[st], b.list_xyzq + e0, uint32_t(nn) * 16u, &s_bar[st]);
+                bulk_g2s(s_type[st], b.list_type + e0, uint32_t(nn) * 4u, &s_bar[st]);
+            }
+        }
+        gchunk += uint32_t(nch);
+        if (tmo_at >= 0) {
+            if (tid == 0) atomicExch(&w.counters[2], 1);
+            return;
+        }
+        // reciprocal term: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c} (FP64-built),
+        // G_k = Σ_s q_s e^{2 pi i n.d_s}, d_s the site's fractional offset from the bin centre
+        double elr = 0.0;
+        if (charged) {
+            const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
+            for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK) {
+                const int32_t kn = min(PA_KCHUNK, k1 - kb);
+                for (int32_t x = tid; x < kn; x += blockDim.x) {
+                    const int32_t kk = kb + x;
+                    const float n1 = b.kcoef[3 * kk], n2 = b.kcoef[3 * kk + 1], n3 = b.kcoef[3 * kk + 2];
+                    s_kc[3 * x] = n1; s_kc[3 * x + 1] = n2; s_kc[3 * x + 2] = n3;
+                    // phase of the bin centre in turns, exact rational reduced in FP64
+                    double ph = double(n1) * double(cx) + double(n2) * double(cy) + double(n3) * double(cz);
+                    ph -= rint(ph);
+                    double sn, cs;
+                    sincospi(2.0 * ph, &sn, &cs);
+                    const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
+                    // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
+                    s_B[x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
+                }
+                __syncthreads();
+                float acc = 0.f, cacc = 0.f;
+                for (int32_t x = 0; x < kn; ++x) {
+                    const float n1 = s_kc[3 * x], n2 = s_kc[3 * x + 1], n3 = s_kc[3 * x + 2];
+                    float gr = 0.f, gi = 0.f;
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const float ph = fmaf(n3, dfr[3 * s + 2], fmaf(n2, dfr[3 * s + 1], n1 * dfr[3 * s]));
+                        float sn, cs;
+                        sincospif(2.0f * ph, &sn, &cs);
+                        gr = fmaf(gqs[s], cs, gr);
+                        gi = fmaf(gqs[s], sn, gi);
+                    }
+                    const float2 B = s_B[x];
+                    kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
+                }
+                elr += double(acc) - double(cacc);
+                __syncthreads();
+            }
+        }
+        if (active) {
+            const double e = double(elj) - double(clj) + KE * (double(esr) - double(csr) + elr) + b.const_offset[fw];
+            w.dU[li] = e;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_energy64: the plain FP64 form of the reference algorithm (src/energy.jl:42-82): for every
+// atom of the framework one minimum image of pos - r_j, then each site's offset added;
+// LJ and screened Coulomb (CUDA's double erfc) inside the cutoffs; reciprocal cross term with
+// double sincos. Tiles hold survivors of one framework; atoms staged through shared memory.
+// ---------------------------------------------------------------------------------------------
+#define PA_TILE64 128
+#define PA_CHUNK64 128
+
+template <int NS>
+__global__ void __launch_bounds__(PA_TILE64) k_energy64(DevBatch<double> b, CallArgs ca, Work w) {
+    __shared__ double4 s_at[PA_CHUNK64];
+    __shared__ int32_t s_ty[PA_CHUNK64];
+    __shared__ int32_t s_item[4];
+    const int tid = threadIdx.x;
+    const int32_t total_tiles = w.counters[1];
+    const int nt = b.ntypes;
+    for (;;) {
+        if (tid == 0) {
+            int32_t t = atomicAdd(&w.counters[0], 1);
+            s_item[0] = t;
+            if (t < total_tiles) {
+                int32_t bin = find_bin(w.tile_start, b.nbins, t);
+                int32_t lo = w.bin_start[bin] + (t - w.tile_start[bin]) * PA_TILE64;
+                s_item[1] = bin; s_item[2] = lo; s_item[3] = min(lo + PA_TILE64, w.bin_start[bin + 1]);
+            }
+        }
+        __syncthreads();
+        const int32_t t = s_item[0];
+        if (t >= total_tiles) break;
+        const int32_t bin = s_item[1], lo = s_item[2], hi = s_item[3];
+        __syncthreads();
+        const int32_t fw = b.bin_fw[bin];
+        const bool active = lo + tid < hi;
+        const int32_t li = active ? w.sorted[lo + tid] : 0;
+        const double4 pa = active ? w.pose64a[li] : make_double4(0.5, 0.5, 0.5, 0);
+        const double4 pq = active ? w.pose64b[li] : make_double4(0, 0, 0, 1);
+        double A[9], iA[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) { A[r] = b.cells[9 * fw + r]; iA[r] = b.invcells[9 * fw + r]; }
+        const double rp[3] = {pa.x, pa.y, pa.z}, q[4] = {pq.x, pq.y, pq.z, pq.w};
+        double pos[3];
+        matvec_s(A, rp, pos);
+        double gx[NS], gy[NS], gz[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            double g[3];
+            rotate_s(q, b.gsite + 3 * s, g);
+            gx[s] = g[0]; gy[s] = g[1]; gz[s] = g[2];
+        }
+        const double rl2 = b.rl2, re2 = b.re2, alpha = b.alphas[fw];
+        double elj = 0, esr = 0;
+        const int32_t a0 = b.atom_offsets[fw], a1 = b.atom_offsets[fw + 1];
+        for (int32_t c0 = a0; c0 < a1; c0 += PA_CHUNK64) {
+            const int32_t n = min(PA_CHUNK64, a1 - c0);
+            for (int32_t x = tid; x < n; x += blockDim.x) { s_at[x] = b.atoms[c0 + x]; s_ty[x] = b.types[c0 + x]; }
+            __syncthreads();
+            for (int32_t j = 0; j < n; ++j) {
+                const double4 at = s_at[j];
+                double D[3] = {pos[0] - at.x, pos[1] - at.y, pos[2] - at.z};
+                const double f0 = iA[0] * D[0] + iA[3] * D[1] + iA[6] * D[2];
+                const double f1 = iA[1] * D[0] + iA[4] * D[1] + iA[7] * D[2];
+                const double f2 = iA[2] * D[0] + iA[5] * D[1] + iA[8] * D[2];
+                const double r0 = rint(f0), r1 = rint(f1), r2i = rint(f2);
+                D[0] -= A[0] * r0 + A[3] * r1 + A[6] * r2i;
+                D[1] -= A[1] * r0 + A[4] * r1 + A[7] * r2i;
+                D[2] -= A[2] * r0 + A[5] * r1 + A[8] * r2i;
+                const int32_t ty = s_ty[j];
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const double dx = D[0] + gx[s], dy = D[1] + gy[s], dz = D[2] + gz[s];
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < rl2) {
+                        const double sg = b.sig2[s * nt + ty] / r2;
+                        const double x3 = sg * sg * sg;
+                        elj += b.eps4[s * nt + ty] * (x3 * x3 - x3);
+                    }
+                    if (r2 < re2 && b.has_charge) {
+                        const double r = sqrt(r2);
+                        esr += b.gq[s] * at.w * erfc(alpha * r) / r;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        double elr = 0;
+        if (b.has_charge) {
+            for (int32_t kk = b.k_offsets[fw]; kk < b.k_offsets[fw + 1]; ++kk) {
+                const double kx = b.kvec[3 * kk], ky = b.kvec[3 * kk + 1], kz = b.kvec[3 * kk + 2];
+                double gr = 0, gi = 0;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double sn, cs;
+                    sincos(kx * (pos[0] + gx[s]) + ky * (pos[1] + gy[s]) + kz * (pos[2] + gz[s]), &sn, &cs);
+                    gr += b.gq[s] * cs; gi += b.gq[s] * sn;
+                }
+                elr += b.kS2[2 * kk] * gr + b.kS2[2 * kk + 1] * gi;
+            }
+        }
+        if (active) w.dU[li] = elj + KE * (esr + elr) + b.const_offset[fw];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_segsum: per segment, x_i = -ΔU_i/kT; m = max x; Σ exp(x - m); Σ ΔU exp(x - m) (terms whose
+// weight is exactly zero contribute zero, as in boltzmann_weight). 256 threads, 8 consecutive
+// insertions per thread summed in order, then a fixed shuffle/shared-memory tree.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_segsum(Work w, double kT) {
+    __shared__ double s_red[3][8];
+    const int64_t b0 = w.seg_rng[2 * blockIdx.x], b1 = w.seg_rng[2 * blockIdx.x + 1];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = PA_SEGMENT_SIZE / 256;
+    const double NEG_INF = __longlong_as_double(0xfff0000000000000LL);
+    double xs[per], us[per];
+    double m = NEG_INF;
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+        const int64_t i = b0 + int64_t(tid) * per + q;
+        double u = i < b1 ? w.dU[i] : __longlong_as_double(0x7ff0000000000000LL);
+        double x = -u / kT;
+        xs[q] = x; us[q] = u;
+        m = fmax(m, x);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) s_red[0][wid] = m;
+    __syncthreads();
+    m = s_red[0][0];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) m = fmax(m, s_red[0][q]);
+    __syncthreads();
+    double sw = 0, su = 0;
+    if (m != NEG_INF && !isnan(m)) {
+#pragma unroll
+        for (int q = 0; q < per; ++q) {
+            const double e = exp(xs[q] - m);
+            if (e != 0.0) { sw += e; su += us[q] * e; }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sw += __shfl_xor_sync(0xffffffffu, sw, o);
+        su += __shfl_xor_sync(0xffffffffu, su, o);
+    }
+    if (lane == 0) { s_red[1][wid] = sw; s_red[2][wid] = su; }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0, c = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) { a += s_red[1][q]; c += s_red[2][q]; }
+        w.seg_out[3 * blockIdx.x] = m;
+        w.seg_out[3 * blockIdx.x + 1] = a;
+        w.seg_out[3 * blockIdx.x + 2] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Neighbour lists of the FP32 path: for bin centre c (fractional, FP32-defined) and atom j with
+// fractional position f_j, every image A (f_j - c - round(f_j - c) + n), n in [-m, m]^3, within
+// radius R is one entry, stored relative to the bin centre. Order: atom index, then n (x fastest),
+// so the lists (and every energy sum over them) are deterministic. One CTA per bin.
+// ---------------------------------------------------------------------------------------------
+struct ListGeom {
+    const double* frac;        // 3*natoms fractional coordinates (cell-sorted order)
+    const double* charges;     // natoms
+    const int32_t* types;      // natoms, 0-based
+    const double* cells;       // 9*nfw
+    const int32_t* atom_offsets;
+    const int32_t* bin_dims;   // 3*nfw
+    const int32_t* bin_base;   // nfw+1
+    const int32_t* bin_fw;     // nbins
+    const double* radius2;     // nfw
+    const int32_t* nimg;       // nfw: m
+    int32_t* counts;           // nbins (count pass)
+    const int32_t* offsets;    // nbins+1 (fill pass)
+    float4* xyzq;
+    int32_t* type_out;
+};
+
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_lists(ListGeom g) {
+    __shared__ int32_t s_warp[8];
+    __shared__ int32_t s_base;
+    const int32_t bin = blockIdx.x, fw = g.bin_fw[bin];
+    const int32_t* nb = g.bin_dims + 3 * fw;
+    const int32_t lb = bin - g.bin_base[fw];
+    const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
+    const double c[3] = {double(__fdiv_rn(float(bx) + 0.5f, float(nb[0]))),
+                         double(__fdiv_rn(float(by) + 0.5f, float(nb[1]))),
+                         double(__fdiv_rn(float(bz) + 0.5f, float(nb[2])))};
+    const double* A = g.cells + 9 * fw;
+    const double R2 = g.radius2[fw];
+    const int32_t m = g.nimg[fw], side = 2 * m + 1, nimgs = side * side * side;
+    const int32_t a0 = g.atom_offsets[fw], a1 = g.atom_offsets[fw + 1];
+    const int64_t npairs = int64_t(a1 - a0) * nimgs;
+    if (threadIdx.x == 0) s_base = FILL ? g.offsets[bin] : 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t p0 = 0; p0 < npairs; p0 += blockDim.x) {
+        const int64_t p = p0 + threadIdx.x;
+        bool keep = false;
+        double dx = 0, dy = 0, dz = 0;
+        int32_t j = 0;
+        if (p < npairs) {
+            j = a0 + int32_t(p / nimgs);
+            const int32_t im = int32_t(p % nimgs);
+            const int32_t n0 = im % side - m, n1 = (im / side) % side - m, n2 = im / (side * side) - m;
+            double d0 = St<double>::sub(g.frac[3 * j], c[0]), d1 = St<double>::sub(g.frac[3 * j + 1], c[1]),
+                   d2 = St<double>::sub(g.frac[3 * j + 2], c[2]);
+            // strict operations: the count and fill instantiations must keep identical sets
+            typedef St<double> S;
+            d0 = S::add(S::sub(d0, rint(d0)), double(n0));
+            d1 = S::add(S::sub(d1, rint(d1)), double(n1));
+            d2 = S::add(S::sub(d2, rint(d2)), double(n2));
+            dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
+            dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
+            dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
+            keep = dot3s(dx, dy, dz, dx, dy, dz) <= R2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_warp[wid] = __popc(bal);
+        __syncthreads();
+        int32_t before = 0, tot = 0;
+        for (int q = 0; q < 8; ++q) { int32_t v = s_warp[q]; if (q < wid) before += v; tot += v; }
+        if (FILL && keep) {
+            const int32_t pos = s_base + before + __popc(bal & ((1u << lane) - 1u));
+            if (pos < g.offsets[bin + 1]) {
+                g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
+                g.type_out[pos] = g.types[j];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += tot;
+        __syncthreads();
+    }
+    if (!FILL && threadIdx.x == 0) g.counts[bin] = s_base;
+    if (FILL) {  // padding entries up to the next offset: far away, no charge
+        const int32_t end = g.offsets[bin + 1];
+        for (int32_t q = s_base + threadIdx.x; q < end; q += blockDim.x) {
+            g.xyzq[q] = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.0f);
+            g.type_out[q] = 0;
+        }
+    }
+}
+
+// FP64 structure factor: one thread per k-vector, sequential sum over atoms (src/ewald.jl:159-170).
+__global__ void __launch_bounds__(256) k_structure_factor(const double* ks, int64_t nk, const double* pos,
+                                                          const double* q, int64_t na, double* S) {
+    __shared__ double4 s_a[256];
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double kx = 0, ky = 0, kz = 0;
+    if (i < nk) { kx = ks[3 * i]; ky = ks[3 * i + 1]; kz = ks[3 * i + 2]; }
+    double re = 0, im = 0;
+    for (int64_t c0 = 0; c0 < na; c0 += 256) {
+        const int64_t n = (na - c0) < 256 ? (na - c0) : 256;
+        if (threadIdx.x < n) {
+            const int64_t j = c0 + threadIdx.x;
+            s_a[threadIdx.x] = make_double4(pos[3 * j], pos[3 * j + 1], pos[3 * j + 2], q[j]);
+        }
+        __syncthreads();
+        for (int64_t j = 0; j < n; ++j) {
+            const double4 a = s_a[j];
+            double sn, cs;
+            sincos(kx * a.x + ky * a.y + kz * a.z, &sn, &cs);
+            re += a.w * cs; im += a.w * sn;
+        }
+        __syncthreads();
+    }
+    if (i < nk) { S[2 * i] = re; S[2 * i + 1] = im; }
+}
+
+}  // namespace pa

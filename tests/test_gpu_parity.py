@@ -1,0 +1,154 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, on a B200.
+
+Tolerances (stated here, used below):
+- poses and phase-0 flags: bit-exact (both follow the same strict operation sequence);
+- FP64 plain path: per-insertion dU rtol 1e-12 (the reference's insertion_energy vs brute-force
+  bound, test/energy_tests.jl:115); results rtol 1e-10 (test/gpu_tests.jl:20-22);
+- FP32 path: per-insertion |dU32 - dU64| <= 1e-5 |dU64| + 2e-6 eV (FP32 pair terms of up to
+  ~1 eV summed over ~1,700 in-cutoff pairs); aggregate |Δ ln K_H| <= 1e-3 and
+  |Δ q_st| <= 5.18e-4 eV (0.05 kJ/mol) against the all-FP64 oracle on the same stream.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import kT_of, oracle_view
+
+pytestmark = pytest.mark.gpu
+
+F32_REL, F32_ABS = 1e-5, 2e-6
+
+
+def run_both(pa, orc, batch, guest, ninsert, seed, nblocks, reject=True, backend=None, T=298.15):
+    ins = {}
+    res = pa._widom(batch, guest, reject=reject, T=T, ninsert=ninsert, seed=seed, nblocks=nblocks,
+                    insertions=ins, backend=backend)
+    v, keep = oracle_view(orc, batch)
+    kT = kT_of(pa, batch, T)
+    rho2, reach0 = pa.build_rejection_tables(batch, kT) if reject else (None, None)
+    prec = 32 if batch.T == np.float32 else 64
+    run = pa.default_run(ninsert, batch.nsys)
+    ref = orc.widom(v, prec, kT, ninsert, seed, nblocks, run, reject, rho2, reach0)
+    return res, ins, ref, kT
+
+
+def ref_results(pa, batch, ref, kT, nblocks):
+    Vf = batch.volumes.astype(batch.T).astype(np.float64)
+    return [pa._reduce(ref["sW"][s], ref["sUW"][s], ref["n"][s], kT, Vf[batch.framework_of[s] - 1], s + 1)
+            for s in range(batch.nsys)]
+
+
+@pytest.fixture(scope="module")
+def co2_small(pa):
+    fws, ff, guest, ewald, _ = pa.synthetic.co2()
+    return fws, ff, guest, ewald
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+def test_poses_flags_energies_co2(pa, orc, backend, co2_small, T):
+    fws, ff, guest, ewald = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=T)
+    res, ins, ref, kT = run_both(pa, orc, batch, guest, 20_000, 5, 4, backend=backend)
+    assert np.array_equal(ins["poses"], ref["poses"])
+    assert np.array_equal(ins["flags"], ref["flags"])
+    surv = ref["flags"] == 0
+    assert np.all(np.isinf(ins["dU"][~surv]))
+    a, b = ins["dU"][surv], ref["dU"][surv]
+    if T == np.float64:
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=0)
+        for r, q in zip(res, ref_results(pa, batch, ref, kT, 4)):
+            for f in ("mu_ex", "K_H", "q_st", "mu_ex_err", "K_H_err", "q_st_err"):
+                assert getattr(r, f) == pytest.approx(getattr(q, f), rel=1e-10)
+    else:
+        err = np.abs(a - b)
+        assert np.all(err <= F32_REL * np.abs(b) + F32_ABS), f"max err {err.max()}"
+        for r, q in zip(res, ref_results(pa, batch, ref, kT, 4)):
+            assert abs(math.log(r.K_H) - math.log(q.K_H)) <= 1e-3
+            assert abs(r.q_st - q.q_st) <= 5.18e-4
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+def test_two_phase_equals_single_phase(pa, backend, co2_small, T):
+    fws, ff, guest, ewald = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=T)
+    r2 = pa.widom(batch, guest, T=298.15, ninsert=6000, seed=17, nblocks=4, chunk=4, backend=backend)
+    r1 = pa.widom_singlephase(batch, guest, T=298.15, ninsert=6000, seed=17, nblocks=4, chunk=4, backend=backend)
+    assert r1 == r2
+
+
+def test_lj_ch4_parity(pa, orc, backend):
+    fws, ff, guest, ewald, prm = pa.synthetic.lj_ch4()
+    for T in (np.float64, np.float32):
+        batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=T)
+        res, ins, ref, kT = run_both(pa, orc, batch, guest, 30_000, 42, 10, backend=backend)
+        assert np.array_equal(ins["flags"], ref["flags"])
+        surv = ref["flags"] == 0
+        a, b = ins["dU"][surv], ref["dU"][surv]
+        if T == np.float64:
+            np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-15)
+        else:
+            assert np.all(np.abs(a - b) <= F32_REL * np.abs(b) + F32_ABS)
+
+
+def test_batched_frameworks_parity(pa, orc, backend):
+    fws, ff, guest, ewald, _ = pa.synthetic.batched(nfw=4, max_unit_atoms=300)
+    for T in (np.float64, np.float32):
+        batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=T)
+        res, ins, ref, kT = run_both(pa, orc, batch, guest, 16_000, 7, 4, backend=backend)
+        assert np.array_equal(ins["poses"], ref["poses"])
+        assert np.array_equal(ins["flags"], ref["flags"])
+        surv = ref["flags"] == 0
+        a, b = ins["dU"][surv], ref["dU"][surv]
+        if T == np.float64:
+            np.testing.assert_allclose(a, b, rtol=1e-12)
+        else:
+            assert np.all(np.abs(a - b) <= F32_REL * np.abs(b) + F32_ABS)
+
+
+def test_empty_box_ideal_gas(pa, backend):
+    A = pa.cell_matrix(30.0, 30.0, 30.0, 90, 90, 90)
+    fw = pa.Framework(A, np.zeros((0, 3)), [], [], np.zeros(0))
+    ff = pa.ForceField(["X_"], [3.0], [0.001], cutoff=12.0, tail=False)
+    g = pa.Guest(np.zeros((1, 3)), [1], np.zeros(1))
+    for T in (np.float64, np.float32):
+        b = pa.FrameworkBatch([fw], ff, g, pa.EwaldParams(cutoff=12.0), T=T)
+        r = pa.widom(b, g, T=300.0, ninsert=10_000, seed=1, backend=backend)[0]
+        kT = float(T(pa.KB * 300.0))
+        assert abs(r.mu_ex) < 1e-12
+        assert r.K_H == pytest.approx(float(T(30.0**3)) / kT, rel=1e-6)
+        assert r.q_st == pytest.approx(kT)
+        assert r.nsamples == 10_000
+
+
+def test_sharded_segments_combine_exactly(pa, backend, co2_small):
+    fws, ff, guest, ewald = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32)
+    ninsert, nblocks = 40_000, 4
+    run = pa.default_run(ninsert, 1)
+    full = pa.widom(batch, guest, T=298.15, ninsert=ninsert, seed=9, nblocks=nblocks, backend=backend)
+    nseg = pa._lib.ctypes.c_int64()
+    pa._lib.lib().pa_segment_count(ninsert, 1, run, nblocks, pa._lib.ctypes.byref(nseg))
+    segs = np.zeros(3 * nseg.value)
+    cut = nseg.value // 3
+    for rng in ((0, cut), (cut, nseg.value)):
+        pa._widom(batch, guest, reject=True, T=298.15, ninsert=ninsert, seed=9, nblocks=nblocks, backend=backend,
+                  segment_range=rng, segments_out=segs)
+    lse, sw, suw = np.zeros(nblocks), np.zeros(nblocks), np.zeros(nblocks)
+    cnt = np.zeros(nblocks, dtype=np.int64)
+    sums = pa._lib.BlockSums(*(pa._lib.ptr(a) for a in (lse, sw, suw, cnt)), None)
+    assert pa._lib.lib().pa_combine_segments(ninsert, 1, run, nblocks, pa._lib.ptr(segs), sums) == 0
+    kT = kT_of(pa, batch)
+    sW, sUW = pa.block_sums(lse, sw, suw)
+    combined = pa._reduce(sW, sUW, cnt, kT, float(np.float32(batch.volumes[0])), 1)
+    assert combined == full[0]
+
+
+def test_device_structure_factor(pa, backend, co2_small):
+    fws, ff, guest, ewald = co2_small
+    fw = fws[0]
+    ks, w, c = pa.kvectors(fw.cell, 1.0)
+    pos = pa.cartesian(fw)
+    S_host = pa.structure_factor(ks, pos, fw.charges)
+    S_dev = backend.ctx.structure_factor(ks, pos, fw.charges)
+    np.testing.assert_allclose(S_dev, S_host, rtol=1e-10, atol=1e-10)
