@@ -1,8 +1,10 @@
 """ctypes binding to the C ABI in include/pureadsorb_b200.h (libpureadsorb_b200.so, built
 in-tree by build.py). Every call checks its status and raises with the library's message; a
 missing library raises LibraryMissing: there is no fallback path."""
+import atexit
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -73,6 +75,17 @@ SIGNATURES = [
 ]
 
 _lib = None
+# live library objects, released in dependency order (batches, then contexts) before the
+# interpreter shuts the CUDA runtime down
+_live_contexts = weakref.WeakSet()
+
+
+def _release_all():
+    for ctx in list(_live_contexts):
+        ctx.close()
+
+
+atexit.register(_release_all)
 
 
 def lib():
@@ -119,6 +132,8 @@ class Context:
             raise PAError(st, f"pa_context_create(device={device}) failed (is a CUDA device visible?)")
         self.handle = h.value
         self.device = device
+        self.batches = weakref.WeakSet()
+        _live_contexts.add(self)
 
     def check(self, st, what):
         if st != PA_OK:
@@ -126,6 +141,9 @@ class Context:
             raise PAError(st, f"{what}: {msg.decode() if msg else ''}")
 
     def close(self):
+        """Frees this context's batches, then the context."""
+        for b in list(getattr(self, "batches", ())):
+            b.free()
         if self.handle:
             lib().pa_context_destroy(self.handle)
             self.handle = None
@@ -169,6 +187,7 @@ class DeviceBatch:
         self.handle = h.value
         self.precision = precision
         self._keep = keep
+        ctx.batches.add(self)
 
     def info(self):
         a, b = _i64(), _i64()

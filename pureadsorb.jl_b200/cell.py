@@ -36,8 +36,15 @@ def cell_matrix(a, b, c, alpha, beta, gamma):
     return np.array([[a, b * cg, c * cb], [0.0, b * sg, c * cy], [0.0, 0.0, c * cz]])
 
 
+def det3(A):
+    """Cofactor expansion along the first row (exact for diagonal and triangular cells, unlike
+    an LU-based determinant)."""
+    return float(A[0, 0] * (A[1, 1] * A[2, 2] - A[1, 2] * A[2, 1]) - A[0, 1] * (A[1, 0] * A[2, 2] - A[1, 2] * A[2, 0])
+                 + A[0, 2] * (A[1, 0] * A[2, 1] - A[1, 1] * A[2, 0]))
+
+
 def volume(A):
-    return abs(float(np.linalg.det(A)))
+    return abs(det3(A))
 
 
 def perpendicular_lengths(A):

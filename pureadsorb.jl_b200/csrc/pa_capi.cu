@@ -58,7 +58,8 @@ struct pa_context {
 };
 
 struct pa_batch {
-    pa_context* ctx = nullptr;
+    pa_context* ctx = nullptr;  // the uploading context; only compared, never dereferenced on free
+    int32_t device = 0;
     int32_t precision = 0;
     int32_t nsys = 0, nfw = 0, ntypes = 0, nguest = 0, nbins = 0;
     int64_t natoms = 0, nk = 0, list_entries = 0;
@@ -490,7 +491,7 @@ pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t pr
         if (desc->guest_types[a] < 1 || desc->guest_types[a] > desc->ntypes) return fail(ctx, PA_ERR_ARG, "guest type out of range");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
     pa_batch* B = new pa_batch();
-    B->ctx = ctx; B->precision = precision;
+    B->ctx = ctx; B->device = ctx->device; B->precision = precision;
     B->nsys = desc->nsys; B->nfw = nfw; B->ntypes = desc->ntypes; B->nguest = desc->nguest;
     B->natoms = na; B->nk = nk;
     B->framework_of.assign(desc->framework_of, desc->framework_of + desc->nsys);
@@ -503,10 +504,12 @@ pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t pr
     return PA_OK;
 }
 
+// Frees a batch. Independent of the context's lifetime (the context may already be destroyed):
+// it waits for the device, then releases the batch's memory.
 pa_status pa_batch_free(pa_batch* batch) {
     if (!batch) return PA_ERR_ARG;
-    cudaSetDevice(batch->ctx->device);
-    cudaStreamSynchronize(batch->ctx->stream);
+    cudaSetDevice(batch->device);
+    cudaDeviceSynchronize();
     delete batch;
     return PA_OK;
 }
