@@ -243,7 +243,13 @@ def main():
         L = list_entries / nbins
         N = len(batch.guest_types)
         nk = int(batch.k_offsets[1])
-        flops_surv = 8 * N * L + 10 * n_lj + 38 * n_ew + 29 * N * nk + 6 * nk
+        kc = batch.kcoeffs
+        rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
+        # executed FP32 work of k_energy32 per survivor (FMA = 2 flops; model stated in DESIGN.md):
+        # 8 per (list entry, site) distance, 52 per in-cutoff pair (LJ 10 + screened Coulomb 38 +
+        # compensated add 4), 10 per (k, site) + 7 per k for the reciprocal recurrence, 25 per
+        # (row start, site) for the direct phase evaluation
+        flops_surv = 8 * N * L + 52 * n_lj + (10 * N + 7) * nk + 25 * N * rows
         e_ms = kms[2] / max(1, kn[2])
         surv_per_launch = surv_frac * (s1 - s0) * (ninsert / nseg)
         achieved = flops_surv * surv_per_launch / (e_ms / 1e3) / 1e12

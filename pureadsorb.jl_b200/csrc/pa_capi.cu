@@ -65,7 +65,7 @@ struct pa_batch {
     int64_t natoms = 0, nk = 0, list_entries = 0;
     std::vector<int32_t> framework_of, atom_offsets, k_offsets;
     DevMem framework_of_d, cells, invcells, alphas, const_offset, atom_offsets_d, atoms, types, ncells,
-        cell_offsets, cellgrid_offsets, k_offsets_d, kvec, kcoef, kS2, sig2, eps4, bin_dims, bin_base, bin_fw,
+        cell_offsets, cellgrid_offsets, k_offsets_d, kvec, kcoef, kstep, kS2, sig2, eps4, bin_dims, bin_base, bin_fw,
         list_offsets, list_xyzq, list_type;
     pa::DevBatch<float> d32{};
     pa::DevBatch<double> d64{};
@@ -197,7 +197,7 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     d.types = B->types.as<int32_t>();
     d.ncells = B->ncells.as<int32_t>(); d.cell_offsets = B->cell_offsets.as<int32_t>();
     d.cellgrid_offsets = B->cellgrid_offsets.as<int32_t>();
-    d.k_offsets = B->k_offsets_d.as<int32_t>(); d.kvec = B->kvec.as<double>(); d.kcoef = B->kcoef.as<float>();
+    d.k_offsets = B->k_offsets_d.as<int32_t>(); d.kvec = B->kvec.as<double>(); d.kcoef4 = B->kcoef.as<float4>(); d.kstep = B->kstep.as<float>();
     d.kS2 = B->kS2.as<double>();
     d.sig2 = B->sig2.as<F>(); d.eps4 = B->eps4.as<F>();
     d.has_charge = 0;
@@ -233,20 +233,38 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     std::vector<int32_t> coff(desc->cell_offsets, desc->cell_offsets + ncoff);
     std::vector<int32_t> cgo(desc->cellgrid_offsets, desc->cellgrid_offsets + nfw + 1);
     std::vector<double> kvec(desc->ks, desc->ks + 3 * nk), kS2(2 * nk);
-    std::vector<float> kcoef(3 * nk);
+    std::vector<float4> kcoef4(nk);
+    std::vector<float> kstep(nfw, 1.0f);
     for (int64_t i = 0; i < nk; ++i) {
         kS2[2 * i] = 2 * desc->kprefactor[i] * desc->Shost[2 * i];
         kS2[2 * i + 1] = 2 * desc->kprefactor[i] * desc->Shost[2 * i + 1];
     }
-    for (int fw = 0; fw < nfw; ++fw)
-        for (int32_t i = B->k_offsets[fw]; i < B->k_offsets[fw + 1]; ++i)
+    for (int fw = 0; fw < nfw; ++fw) {
+        const int32_t k0 = B->k_offsets[fw], k1 = B->k_offsets[fw + 1];
+        std::vector<int32_t> n(3 * (k1 - k0));
+        for (int32_t i = k0; i < k1; ++i)
             for (int r = 0; r < 3; ++r) {
-                if (desc->kcoeffs) { kcoef[3 * i + r] = float(desc->kcoeffs[3 * i + r]); continue; }
+                if (desc->kcoeffs) { n[3 * (i - k0) + r] = desc->kcoeffs[3 * i + r]; continue; }
                 // n_r = a_r . k / (2 pi), a_r the r-th lattice vector (column r of A)
                 const double* A = desc->cells + 9 * fw;
                 double v = (A[3 * r] * kvec[3 * i] + A[3 * r + 1] * kvec[3 * i + 1] + A[3 * r + 2] * kvec[3 * i + 2]) / (2 * M_PI);
-                kcoef[3 * i + r] = float(std::nearbyint(v));
+                n[3 * (i - k0) + r] = int32_t(std::nearbyint(v));
             }
+        // the row step: smallest positive n3 increment between consecutive k-vectors of equal (n1, n2)
+        int32_t step = 0;
+        for (int32_t q = 1; q < k1 - k0; ++q)
+            if (n[3 * q] == n[3 * q - 3] && n[3 * q + 1] == n[3 * q - 2]) {
+                int32_t d = n[3 * q + 2] - n[3 * q - 1];
+                if (d > 0 && (step == 0 || d < step)) step = d;
+            }
+        if (step == 0) step = 1;
+        kstep[fw] = float(step);
+        for (int32_t q = 0; q < k1 - k0; ++q) {
+            bool cont = q > 0 && n[3 * q] == n[3 * q - 3] && n[3 * q + 1] == n[3 * q - 2] &&
+                        n[3 * q + 2] - n[3 * q - 1] == step;
+            kcoef4[k0 + q] = make_float4(float(n[3 * q]), float(n[3 * q + 1]), float(n[3 * q + 2]), cont ? 1.f : 0.f);
+        }
+    }
     std::vector<F> sig2(N * nt), eps4(N * nt);
     for (int a = 0; a < N; ++a) {
         int gt = desc->guest_types[a] - 1;
@@ -304,7 +322,8 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     PA_CUDA(ctx, upload(B->cellgrid_offsets, cgo, st));
     PA_CUDA(ctx, upload(B->k_offsets_d, B->k_offsets, st));
     PA_CUDA(ctx, upload(B->kvec, kvec, st));
-    PA_CUDA(ctx, upload(B->kcoef, kcoef, st));
+    PA_CUDA(ctx, upload(B->kcoef, kcoef4, st));
+    PA_CUDA(ctx, upload(B->kstep, kstep, st));
     PA_CUDA(ctx, upload(B->kS2, kS2, st));
     PA_CUDA(ctx, upload(B->sig2, sig2, st));
     PA_CUDA(ctx, upload(B->eps4, eps4, st));
@@ -385,7 +404,7 @@ cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::W
             cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
             if (e != cudaSuccess) return e;
         }
-        pa::k_energy32<NS><<<num_sms * 4, PA_TILE32, dyn, st>>>(B->d32, ca, w);
+        pa::k_energy32<NS><<<num_sms * PA_CTAS_PER_SM32, PA_TILE32, dyn, st>>>(B->d32, ca, w);
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }

@@ -44,7 +44,9 @@ struct DevBatch {
     const int32_t* cellgrid_offsets;              // nfw+1
     const int32_t* k_offsets;                     // nfw+1
     const double* kvec;                           // 3*nk Cartesian (FP64 path)
-    const float* kcoef;                           // 3*nk integer coefficients as float (FP32 path)
+    const float4* kcoef4;                         // nk: (n1, n2, n3, 1 if the k-vector continues its
+                                                  //  row of equal (n1, n2) by kstep in n3, else 0)
+    const float* kstep;                           // nfw: n3 step along a row
     const double* kS2;                            // 2*nk: 2*kpref*S_re, 2*kpref*S_im (FP64)
     const F* sig2;                                // nguest*ntypes: sigma^2 of (site, host type)
     const F* eps4;                                // nguest*ntypes: 4 eps
@@ -293,38 +295,42 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // ---------------------------------------------------------------------------------------------
-// FP32 screened Coulomb: erfc(z)/r with z = alpha r, r = sqrt(r2). erfc(z) = exp(-z^2) P(t),
-// t = 2/(2+z), P a degree-9 fit (gen_coeffs.py), ~2e-7 relative on [0, 4].
+// FP32 helpers. rcp_nr: hardware reciprocal estimate refined by one Newton step (about 1 ulp).
+// erfc_over_r: erfc(z)/r with z = alpha r, r = sqrt(r2); erfc(z) = exp(-z^2) P(t), t = 2/(2+z),
+// P a degree-9 fit (gen_coeffs.py), about 2e-7 relative on [0, 4].
 // ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_nr(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return fmaf(r, fmaf(-x, r, 1.0f), r);
+}
 __device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
     float ri = rsqrtf(r2);
     ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);  // one Newton step
-    float r = r2 * ri;
-    float z = alpha * r;
-    float d = fmaf(0.5f, z, 1.0f);
-    float t = __frcp_rn(d);
+    const float z = alpha * (r2 * ri);
+    const float t = rcp_nr(fmaf(0.5f, z, 1.0f));
     const float c[PA_NERFC32] = PA_ERFC32_INIT;
     float p = c[PA_NERFC32 - 1];
 #pragma unroll
     for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, t, c[k]);
-    float e = __expf(-z * z);
-    return p * e * ri;
+    return p * __expf(-z * z) * ri;
 }
 
 // ---------------------------------------------------------------------------------------------
 // k_energy32: persistent CTAs over (bin, tile) items; one insertion per thread.
 // ---------------------------------------------------------------------------------------------
 #define PA_TILE32 128
-#define PA_CHUNK32 256
+#define PA_CHUNK32 512
 #define PA_KCHUNK 256
+#define PA_CTAS_PER_SM32 8
 
 template <int NS>
-__global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
+__global__ void __launch_bounds__(PA_TILE32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[2][PA_CHUNK32];
     __shared__ __align__(128) int32_t s_type[2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ float2 s_B[PA_KCHUNK];
-    __shared__ float s_kc[3 * PA_KCHUNK];
+    __shared__ float4 s_kc[PA_KCHUNK];
     __shared__ int32_t s_item[4];
     extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
     const int tid = threadIdx.x;
@@ -367,8 +373,10 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
                 bulk_g2s(s_type[st], b.list_type + e0, uint32_t(n) * 4u, &s_bar[st]);
             }
         }
-        // this thread's insertion
+        // this thread's insertion; a warp without one skips the arithmetic (it still takes part in
+        // the barriers and the shared-memory staging)
         const bool active = lo + tid < hi;
+        const bool warp_live = __any_sync(0xffffffffu, active);
         const int32_t li = active ? w.sorted[lo + tid] : 0;
         const int32_t* nb = b.bin_dims + 3 * fw;
         const int32_t lb = bin - b.bin_base[fw];
@@ -376,11 +384,12 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
         const float cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
         const float cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
         const float cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
-        float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
-        float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
+        const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
+        const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
         const float* A = b.cells + 9 * fw;
         const float* iA = b.invcells + 9 * fw;
         const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
+        // site positions relative to the bin centre (Cartesian) and their fractional offsets
         float px[NS], py[NS], pz[NS], dfr[3 * NS];
         {
             const float q[4] = {pq.x, pq.y, pq.z, pq.w};
@@ -395,18 +404,18 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
                 float g[3];
                 rotate_s(q, gsb + 3 * s, g);
                 px[s] = c0 + g[0]; py[s] = c1 + g[1]; pz[s] = c2 + g[2];
-                // fractional offset of the site from the bin centre, for the reciprocal term
                 dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
                 dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
                 dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
             }
         }
-        float gqs[NS];
+        float gqs[NS], gqk[NS];  // site charges, and the same times the Coulomb constant
 #pragma unroll
-        for (int s = 0; s < NS; ++s) gqs[s] = b.gq[s];
-        const float rl2 = b.rl2, re2 = b.re2, alpha = float(b.alphas[fw]);
+        for (int s = 0; s < NS; ++s) { gqs[s] = b.gq[s]; gqk[s] = float(KE * double(b.gq[s])); }
+        const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
         const bool charged = b.has_charge != 0;
-        float elj = 0.f, clj = 0.f, esr = 0.f, csr = 0.f;
+        // real-space sum of LJ + KE q q erfc(alpha r)/r pair terms, compensated
+        float esum = 0.f, ecmp = 0.f;
         // tmo_at: chunk whose bulk copy did not arrive in time (-1: none). After a timeout no
         // further copies are issued and only the chunk already in flight is still waited for.
         int32_t tmo_at = -1;
@@ -416,7 +425,7 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
             if (!issued) break;
             const bool late = !mbar_wait_bounded(&s_bar[st], par);
             const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
-            if (tmo_at < 0 && !late) {
+            if (tmo_at < 0 && !late && warp_live) {
 #pragma unroll 2
                 for (int32_t j = 0; j < n; ++j) {
                     const float4 at = s_xyzq[st][j];
@@ -425,13 +434,16 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
                     for (int s = 0; s < NS; ++s) {
                         const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
                         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        if (r2 < rl2) {
-                            const float inv = __frcp_rn(r2);
-                            const float x = s_sig2[s * nt + ty] * inv;
-                            const float x3 = x * x * x;
-                            kahan_add(elj, clj, s_eps4[s * nt + ty] * (x3 * x3 - x3));
+                        if (r2 < rc2) {
+                            float e = 0.f;
+                            if (r2 < rl2) {
+                                const float x = s_sig2[s * nt + ty] * rcp_nr(r2);
+                                const float x3 = x * x * x;
+                                e = s_eps4[s * nt + ty] * (x3 * x3 - x3);
+                            }
+                            if (charged && r2 < re2) e = fmaf(gqk[s] * at.w, erfc_over_r(r2, alpha), e);
+                            kahan_add(esum, ecmp, e);
                         }
-                        if (charged && r2 < re2) kahan_add(esr, csr, gqs[s] * at.w * erfc_over_r(r2, alpha));
                     }
                 }
             }
@@ -450,19 +462,31 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
             if (tid == 0) atomicExch(&w.counters[2], 1);
             return;
         }
-        // reciprocal term: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c} (FP64-built),
-        // G_k = Σ_s q_s e^{2 pi i n.d_s}, d_s the site's fractional offset from the bin centre
+        // Reciprocal term: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c} built in
+        // FP64 per bin, G_k = Σ_s q_s e^{2 pi i n.d_s} with d_s the site's fractional offset from
+        // the bin centre. k-vectors run in rows of equal (n1, n2); along a row n3 advances by the
+        // framework's step, so e^{2 pi i n.d_s} is carried by one complex multiplication per
+        // k-vector and evaluated directly only at row starts.
         double elr = 0.0;
         if (charged) {
             const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
+            float stc[NS], sts[NS], cr[NS], ci[NS];
+            {
+                const float kst = b.kstep[fw];
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
+                    cr[s] = 1.f; ci[s] = 0.f;
+                }
+            }
             for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK) {
                 const int32_t kn = min(PA_KCHUNK, k1 - kb);
                 for (int32_t x = tid; x < kn; x += blockDim.x) {
                     const int32_t kk = kb + x;
-                    const float n1 = b.kcoef[3 * kk], n2 = b.kcoef[3 * kk + 1], n3 = b.kcoef[3 * kk + 2];
-                    s_kc[3 * x] = n1; s_kc[3 * x + 1] = n2; s_kc[3 * x + 2] = n3;
-                    // phase of the bin centre in turns, exact rational reduced in FP64
-                    double ph = double(n1) * double(cx) + double(n2) * double(cy) + double(n3) * double(cz);
+                    const float4 kc = b.kcoef4[kk];
+                    s_kc[x] = kc;
+                    // phase of the bin centre in turns, reduced in FP64
+                    double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
                     ph -= rint(ph);
                     double sn, cs;
                     sincospi(2.0 * ph, &sn, &cs);
@@ -471,29 +495,36 @@ __global__ void __launch_bounds__(PA_TILE32, 4) k_energy32(DevBatch<float> b, Ca
                     s_B[x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
                 }
                 __syncthreads();
-                float acc = 0.f, cacc = 0.f;
-                for (int32_t x = 0; x < kn; ++x) {
-                    const float n1 = s_kc[3 * x], n2 = s_kc[3 * x + 1], n3 = s_kc[3 * x + 2];
-                    float gr = 0.f, gi = 0.f;
+                if (warp_live) {
+                    float acc = 0.f, cacc = 0.f;
+                    for (int32_t x = 0; x < kn; ++x) {
+                        const float4 kc = s_kc[x];
+                        if (kc.w == 0.f) {  // row start: direct evaluation
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        const float ph = fmaf(n3, dfr[3 * s + 2], fmaf(n2, dfr[3 * s + 1], n1 * dfr[3 * s]));
-                        float sn, cs;
-                        sincospif(2.0f * ph, &sn, &cs);
-                        gr = fmaf(gqs[s], cs, gr);
-                        gi = fmaf(gqs[s], sn, gi);
+                            for (int s = 0; s < NS; ++s) {
+                                const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
+                                sincospif(2.0f * ph, &ci[s], &cr[s]);
+                            }
+                        } else {  // next k-vector of the row
+#pragma unroll
+                            for (int s = 0; s < NS; ++s) {
+                                const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
+                                ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
+                                cr[s] = r;
+                            }
+                        }
+                        float gr = 0.f, gi = 0.f;
+#pragma unroll
+                        for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
+                        const float2 B = s_B[x];
+                        kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
                     }
-                    const float2 B = s_B[x];
-                    kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
+                    elr += double(acc) - double(cacc);
                 }
-                elr += double(acc) - double(cacc);
                 __syncthreads();
             }
         }
-        if (active) {
-            const double e = double(elj) - double(clj) + KE * (double(esr) - double(csr) + elr) + b.const_offset[fw];
-            w.dU[li] = e;
-        }
+        if (active) w.dU[li] = double(esum) - double(ecmp) + KE * elr + b.const_offset[fw];
     }
 }
 
