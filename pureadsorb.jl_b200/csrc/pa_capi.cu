@@ -53,7 +53,7 @@ struct pa_context {
     double ms[NCLASS] = {0};
     int64_t launches[NCLASS] = {0};
     // per-call workspace (grow-only)
-    DevMem pose_a, pose_b, bin_of, slot, sorted, dU, bin_count, bin_start, tile_start, counters, seg_out, seg_rng,
+    DevMem pose_a, pose_b, bin_of, slot, sorted, dU, bin_count, fine_start, bin_start, tile_start, counters, seg_out, seg_rng,
         sys_off, rho2, reach0;
 };
 
@@ -64,11 +64,15 @@ struct pa_batch {
     int32_t nsys = 0, nfw = 0, ntypes = 0, nguest = 0, nbins = 0;
     int64_t natoms = 0, nk = 0, list_entries = 0;
     std::vector<int32_t> framework_of, atom_offsets, k_offsets;
-    DevMem framework_of_d, cells, invcells, alphas, const_offset, atom_offsets_d, atoms, types, ncells,
-        cell_offsets, cellgrid_offsets, k_offsets_d, kvec, kcoef, kstep, kS2, sig2, eps4, bin_dims, bin_base, bin_fw,
-        list_offsets, list_xyzq, list_type;
+    // two stream-ordered allocations: the packed static tables, and the neighbour lists
+    void* arena = nullptr;
+    void* lists = nullptr;
     pa::DevBatch<float> d32{};
     pa::DevBatch<double> d64{};
+    ~pa_batch() {
+        if (arena) cudaFreeAsync(arena, 0);
+        if (lists) cudaFreeAsync(lists, 0);
+    }
 };
 
 namespace {
@@ -91,6 +95,23 @@ cudaError_t upload(DevMem& m, const std::vector<T>& v, cudaStream_t st) {
     if (e != cudaSuccess || v.empty()) return e;
     return cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
+
+// Host staging of many small device tables into one buffer (256-byte aligned slots), uploaded
+// with a single copy into one allocation.
+struct Packer {
+    std::vector<char> host;
+    template <typename T> size_t add(const std::vector<T>& v) {
+        size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + std::max<size_t>(v.size() * sizeof(T), 16));
+        if (!v.empty()) std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+    size_t reserve(size_t bytes) {
+        size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + std::max<size_t>(bytes, 16), 0);
+        return off;
+    }
+};
 
 void perpendicular_lengths(const double* A, double* L) {
     auto cross = [](const double* a, const double* b, double* c) {
@@ -185,30 +206,49 @@ pa_status wait_stream(pa_context* ctx) {
     }
 }
 
-template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc) {
+struct Slots {
+    size_t framework_of, cells, invcells, alphas, const_offset, atom_offsets, atoms, types, ncells, cell_offsets,
+        cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, sig2, eps4, bin_dims, bin_base, bin_fw;
+    size_t list_offsets, list_xyzq, list_type;  // offsets inside the list allocation
+};
+
+template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc, const Slots& o) {
+    char* a = static_cast<char*>(B->arena);
+    char* l = static_cast<char*>(B->lists);
     d.nsys = B->nsys; d.nfw = B->nfw; d.ntypes = B->ntypes; d.nguest = B->nguest; d.nbins = B->nbins;
+    d.nsub = sizeof(F) == 4 ? 64 : 1;
     d.rl2 = F(desc->cutoff * desc->cutoff);
     d.re2 = F(desc->ewald_cutoff * desc->ewald_cutoff);
-    d.framework_of = B->framework_of_d.as<int32_t>();
-    d.cells = B->cells.as<F>(); d.invcells = B->invcells.as<F>();
-    d.alphas = B->alphas.as<double>(); d.const_offset = B->const_offset.as<double>();
-    d.atom_offsets = B->atom_offsets_d.as<int32_t>();
-    d.atoms = B->atoms.as<typename pa::Vec4<F>::T>();
-    d.types = B->types.as<int32_t>();
-    d.ncells = B->ncells.as<int32_t>(); d.cell_offsets = B->cell_offsets.as<int32_t>();
-    d.cellgrid_offsets = B->cellgrid_offsets.as<int32_t>();
-    d.k_offsets = B->k_offsets_d.as<int32_t>(); d.kvec = B->kvec.as<double>(); d.kcoef4 = B->kcoef.as<float4>(); d.kstep = B->kstep.as<float>();
-    d.kS2 = B->kS2.as<double>();
-    d.sig2 = B->sig2.as<F>(); d.eps4 = B->eps4.as<F>();
+    d.framework_of = reinterpret_cast<const int32_t*>(a + o.framework_of);
+    d.cells = reinterpret_cast<const F*>(a + o.cells);
+    d.invcells = reinterpret_cast<const F*>(a + o.invcells);
+    d.alphas = reinterpret_cast<const double*>(a + o.alphas);
+    d.const_offset = reinterpret_cast<const double*>(a + o.const_offset);
+    d.atom_offsets = reinterpret_cast<const int32_t*>(a + o.atom_offsets);
+    d.atoms = reinterpret_cast<const typename pa::Vec4<F>::T*>(a + o.atoms);
+    d.types = reinterpret_cast<const int32_t*>(a + o.types);
+    d.ncells = reinterpret_cast<const int32_t*>(a + o.ncells);
+    d.cell_offsets = reinterpret_cast<const int32_t*>(a + o.cell_offsets);
+    d.cellgrid_offsets = reinterpret_cast<const int32_t*>(a + o.cellgrid_offsets);
+    d.k_offsets = reinterpret_cast<const int32_t*>(a + o.k_offsets);
+    d.kvec = reinterpret_cast<const double*>(a + o.kvec);
+    d.kcoef4 = reinterpret_cast<const float4*>(a + o.kcoef);
+    d.kstep = reinterpret_cast<const float*>(a + o.kstep);
+    d.kS2 = reinterpret_cast<const double*>(a + o.kS2);
+    d.sig2 = reinterpret_cast<const F*>(a + o.sig2);
+    d.eps4 = reinterpret_cast<const F*>(a + o.eps4);
     d.has_charge = 0;
-    for (int a = 0; a < B->nguest; ++a) {
-        for (int r = 0; r < 3; ++r) d.gsite[3 * a + r] = F(desc->guest_sites[3 * a + r]);
-        d.gq[a] = F(desc->guest_charges[a]);
-        if (desc->guest_charges[a] != 0) d.has_charge = 1;
+    for (int q = 0; q < B->nguest; ++q) {
+        for (int r = 0; r < 3; ++r) d.gsite[3 * q + r] = F(desc->guest_sites[3 * q + r]);
+        d.gq[q] = F(desc->guest_charges[q]);
+        if (desc->guest_charges[q] != 0) d.has_charge = 1;
     }
-    d.bin_dims = B->bin_dims.as<int32_t>(); d.bin_base = B->bin_base.as<int32_t>(); d.bin_fw = B->bin_fw.as<int32_t>();
-    d.list_offsets = B->list_offsets.as<int32_t>(); d.list_xyzq = B->list_xyzq.as<float4>();
-    d.list_type = B->list_type.as<int32_t>();
+    d.bin_dims = reinterpret_cast<const int32_t*>(a + o.bin_dims);
+    d.bin_base = reinterpret_cast<const int32_t*>(a + o.bin_base);
+    d.bin_fw = reinterpret_cast<const int32_t*>(a + o.bin_fw);
+    d.list_offsets = l ? reinterpret_cast<const int32_t*>(l + o.list_offsets) : nullptr;
+    d.list_xyzq = l ? reinterpret_cast<const float4*>(l + o.list_xyzq) : nullptr;
+    d.list_type = l ? reinterpret_cast<const int32_t*>(l + o.list_type) : nullptr;
 }
 
 template <typename F>
@@ -309,29 +349,18 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         nimg[fw] = int32_t(std::ceil(R / Lmin + 0.5));
     }
     B->nbins = bbase[nfw];
-    PA_CUDA(ctx, upload(B->framework_of_d, fwo, st));
-    PA_CUDA(ctx, upload(B->cells, cells, st));
-    PA_CUDA(ctx, upload(B->invcells, inv, st));
-    PA_CUDA(ctx, upload(B->alphas, alphas, st));
-    PA_CUDA(ctx, upload(B->const_offset, co, st));
-    PA_CUDA(ctx, upload(B->atom_offsets_d, B->atom_offsets, st));
-    PA_CUDA(ctx, upload(B->atoms, atoms, st));
-    PA_CUDA(ctx, upload(B->types, types, st));
-    PA_CUDA(ctx, upload(B->ncells, ncells, st));
-    PA_CUDA(ctx, upload(B->cell_offsets, coff, st));
-    PA_CUDA(ctx, upload(B->cellgrid_offsets, cgo, st));
-    PA_CUDA(ctx, upload(B->k_offsets_d, B->k_offsets, st));
-    PA_CUDA(ctx, upload(B->kvec, kvec, st));
-    PA_CUDA(ctx, upload(B->kcoef, kcoef4, st));
-    PA_CUDA(ctx, upload(B->kstep, kstep, st));
-    PA_CUDA(ctx, upload(B->kS2, kS2, st));
-    PA_CUDA(ctx, upload(B->sig2, sig2, st));
-    PA_CUDA(ctx, upload(B->eps4, eps4, st));
-    PA_CUDA(ctx, upload(B->bin_dims, bdims, st));
-    PA_CUDA(ctx, upload(B->bin_base, bbase, st));
-    PA_CUDA(ctx, upload(B->bin_fw, bfw, st));
-    if (sizeof(F) == 4) {
-        // neighbour lists: count pass, padded offsets on the host, fill pass
+    // one packed upload of every table (and the list build's temporaries)
+    Packer pk;
+    Slots o{};
+    o.framework_of = pk.add(fwo); o.cells = pk.add(cells); o.invcells = pk.add(inv); o.alphas = pk.add(alphas);
+    o.const_offset = pk.add(co); o.atom_offsets = pk.add(B->atom_offsets); o.atoms = pk.add(atoms);
+    o.types = pk.add(types); o.ncells = pk.add(ncells); o.cell_offsets = pk.add(coff);
+    o.cellgrid_offsets = pk.add(cgo); o.k_offsets = pk.add(B->k_offsets); o.kvec = pk.add(kvec);
+    o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.sig2 = pk.add(sig2);
+    o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
+    const bool lists = sizeof(F) == 4;
+    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0;
+    if (lists) {
         std::vector<double> frac(3 * na), q(desc->charges, desc->charges + na);
         for (int fw = 0; fw < nfw; ++fw)
             for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
@@ -340,19 +369,24 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
                     frac[3 * j + r] = iA[r] * desc->positions[3 * j] + iA[r + 3] * desc->positions[3 * j + 1] +
                                       iA[r + 6] * desc->positions[3 * j + 2];
                 }
-        DevMem dfrac, dq, dcells64, dr2, dnimg, dcount;
         std::vector<double> cells64(desc->cells, desc->cells + 9 * nfw);
-        PA_CUDA(ctx, upload(dfrac, frac, st));
-        PA_CUDA(ctx, upload(dq, q, st));
-        PA_CUDA(ctx, upload(dcells64, cells64, st));
-        PA_CUDA(ctx, upload(dr2, radius2, st));
-        PA_CUDA(ctx, upload(dnimg, nimg, st));
-        PA_CUDA(ctx, dcount.ensure(sizeof(int32_t) * std::max(1, B->nbins)));
+        t_frac = pk.add(frac); t_q = pk.add(q); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
+        t_nimg = pk.add(nimg); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
+    }
+    PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.host.size(), st));
+    PA_CUDA(ctx, cudaMemcpyAsync(B->arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
+    char* base = static_cast<char*>(B->arena);
+    if (lists) {
+        // neighbour lists: count pass, padded offsets on the host, fill pass
         pa::ListGeom g{};
-        g.frac = dfrac.as<double>(); g.charges = dq.as<double>(); g.types = B->types.as<int32_t>();
-        g.cells = dcells64.as<double>(); g.atom_offsets = B->atom_offsets_d.as<int32_t>();
-        g.bin_dims = B->bin_dims.as<int32_t>(); g.bin_base = B->bin_base.as<int32_t>(); g.bin_fw = B->bin_fw.as<int32_t>();
-        g.radius2 = dr2.as<double>(); g.nimg = dnimg.as<int32_t>(); g.counts = dcount.as<int32_t>();
+        g.frac = reinterpret_cast<const double*>(base + t_frac); g.charges = reinterpret_cast<const double*>(base + t_q);
+        g.types = reinterpret_cast<const int32_t*>(base + o.types); g.cells = reinterpret_cast<const double*>(base + t_cells);
+        g.atom_offsets = reinterpret_cast<const int32_t*>(base + o.atom_offsets);
+        g.bin_dims = reinterpret_cast<const int32_t*>(base + o.bin_dims);
+        g.bin_base = reinterpret_cast<const int32_t*>(base + o.bin_base);
+        g.bin_fw = reinterpret_cast<const int32_t*>(base + o.bin_fw);
+        g.radius2 = reinterpret_cast<const double*>(base + t_r2); g.nimg = reinterpret_cast<const int32_t*>(base + t_nimg);
+        g.counts = reinterpret_cast<int32_t*>(base + t_count);
         if (B->nbins > 0) {
             Timer tm(ctx, 4);
             pa::k_lists<false><<<B->nbins, 256, 0, st>>>(g);
@@ -361,7 +395,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         }
         std::vector<int32_t> counts(B->nbins);
         if (B->nbins > 0)
-            PA_CUDA(ctx, cudaMemcpyAsync(counts.data(), dcount.p, sizeof(int32_t) * B->nbins, cudaMemcpyDeviceToHost, st));
+            PA_CUDA(ctx, cudaMemcpyAsync(counts.data(), g.counts, sizeof(int32_t) * B->nbins, cudaMemcpyDeviceToHost, st));
         pa_status ws = wait_stream(ctx);
         if (ws != PA_OK) return ws;
         std::vector<int32_t> loff(B->nbins + 1, 0);
@@ -371,20 +405,27 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             loff[q2 + 1] = loff[q2] + int32_t(padded);
         }
         B->list_entries = loff[B->nbins];
-        PA_CUDA(ctx, upload(B->list_offsets, loff, st));
-        PA_CUDA(ctx, B->list_xyzq.ensure(sizeof(float4) * std::max<int64_t>(1, B->list_entries)));
-        PA_CUDA(ctx, B->list_type.ensure(sizeof(int32_t) * std::max<int64_t>(1, B->list_entries)));
-        g.offsets = B->list_offsets.as<int32_t>(); g.xyzq = B->list_xyzq.as<float4>(); g.type_out = B->list_type.as<int32_t>();
+        Packer lp;
+        o.list_offsets = lp.add(loff);
+        o.list_xyzq = lp.reserve(sizeof(float4) * size_t(std::max<int64_t>(1, B->list_entries)));
+        o.list_type = lp.reserve(sizeof(int32_t) * size_t(std::max<int64_t>(1, B->list_entries)));
+        PA_CUDA(ctx, cudaMallocAsync(&B->lists, lp.host.size(), st));
+        // only the offsets need the host copy; the entries are written by the fill pass
+        PA_CUDA(ctx, cudaMemcpyAsync(B->lists, lp.host.data(), o.list_xyzq, cudaMemcpyHostToDevice, st));
+        char* lb = static_cast<char*>(B->lists);
+        g.offsets = reinterpret_cast<const int32_t*>(lb + o.list_offsets);
+        g.xyzq = reinterpret_cast<float4*>(lb + o.list_xyzq);
+        g.type_out = reinterpret_cast<int32_t*>(lb + o.list_type);
         if (B->nbins > 0) {
             Timer tm(ctx, 4);
             pa::k_lists<true><<<B->nbins, 256, 0, st>>>(g);
             tm.stop(1);
             PA_CUDA(ctx, cudaGetLastError());
         }
-        ws = wait_stream(ctx);  // the temporaries above are freed on return
+        ws = wait_stream(ctx);
         if (ws != PA_OK) return ws;
     }
-    fill_batch_view(B, view<F>(B), desc);
+    fill_batch_view(B, view<F>(B), desc, o);
     return wait_stream(ctx);
 }
 
@@ -404,7 +445,7 @@ cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::W
             cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
             if (e != cudaSuccess) return e;
         }
-        pa::k_energy32<NS><<<num_sms * PA_CTAS_PER_SM32, PA_TILE32, dyn, st>>>(B->d32, ca, w);
+        pa::k_energy32<NS><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
@@ -439,6 +480,13 @@ pa_status pa_context_create(int32_t device, pa_context** out) {
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    // batch tables come from the device's stream-ordered pool; keep freed blocks cached in it so
+    // that repeated uploads reuse memory instead of returning to the driver allocator
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
     ctx->stream = ctx->own;
     *out = ctx;
@@ -518,7 +566,11 @@ pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t pr
     B->k_offsets.assign(desc->k_offsets, desc->k_offsets + nfw + 1);
     pa_status st = precision == PA_PRECISION_F32 ? upload_impl<float>(ctx, desc, B) : upload_impl<double>(ctx, desc, B);
     if (ctx->timing) Timer::collect(ctx);
-    if (st != PA_OK) { delete B; return st; }
+    if (st != PA_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        delete B;
+        return st;
+    }
     *out = B;
     return PA_OK;
 }
@@ -581,7 +633,11 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     PA_CUDA(ctx, ctx->slot.ensure(sizeof(int32_t) * n_act));
     PA_CUDA(ctx, ctx->sorted.ensure(sizeof(int32_t) * n_act));
     PA_CUDA(ctx, ctx->dU.ensure(sizeof(double) * n_act));
-    PA_CUDA(ctx, ctx->bin_count.ensure(sizeof(int32_t) * (B->nbins + 1)));
+    const int32_t nsub = f32 ? 64 : 1;
+    const int64_t nfine = int64_t(B->nbins) * nsub;
+    if (nfine + 1 > INT32_MAX) return fail(ctx, PA_ERR_ARG, "too many spatial bins");
+    PA_CUDA(ctx, ctx->bin_count.ensure(sizeof(int32_t) * (nfine + 1)));
+    PA_CUDA(ctx, ctx->fine_start.ensure(sizeof(int32_t) * (nfine + 1)));
     PA_CUDA(ctx, ctx->bin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
     PA_CUDA(ctx, ctx->tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
     PA_CUDA(ctx, ctx->counters.ensure(sizeof(int32_t) * 8));
@@ -595,13 +651,13 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         if (f32) { std::vector<float> r2(nr); for (int64_t q = 0; q < nr; ++q) r2[q] = float(args->rho2[q]); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
         else { std::vector<double> r2(args->rho2, args->rho2 + nr); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
     }
-    PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (B->nbins + 1), st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
     PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 8, st));
     pa::Work w{};
     if (f32) { w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>(); }
     else { w.pose64a = ctx->pose_a.as<double4>(); w.pose64b = ctx->pose_b.as<double4>(); }
     w.bin_of = ctx->bin_of.as<int32_t>(); w.slot = ctx->slot.as<int32_t>(); w.sorted = ctx->sorted.as<int32_t>();
-    w.dU = ctx->dU.as<double>(); w.bin_count = ctx->bin_count.as<int32_t>(); w.bin_start = ctx->bin_start.as<int32_t>();
+    w.dU = ctx->dU.as<double>(); w.bin_count = ctx->bin_count.as<int32_t>(); w.fine_start = ctx->fine_start.as<int32_t>(); w.bin_start = ctx->bin_start.as<int32_t>();
     w.tile_start = ctx->tile_start.as<int32_t>(); w.counters = ctx->counters.as<int32_t>();
     w.seg_out = ctx->seg_out.as<double>(); w.seg_rng = ctx->seg_rng.as<int64_t>();
     pa::CallArgs ca{};
@@ -616,7 +672,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     }
     {
         Timer tm(ctx, 1);
-        pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, f32 ? PA_TILE32 : PA_TILE64);
+        pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
         pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
         tm.stop(2);
         PA_CUDA(ctx, cudaGetLastError());

@@ -6,10 +6,11 @@
 //               spatial bin plus a slot in it (src/widom.jl:99-151, 399-415);
 //   k_scan      one CTA: exclusive scans of the bin counts and of the per-bin tile counts;
 //   k_scatter   survivors into bin-sorted order;
-//   k_energy32  persistent CTAs over (bin, tile) work items: the bin's imaged neighbour list is
-//               streamed into shared memory by bulk copies (cp.async.bulk + mbarrier, double
-//               buffered), one insertion per thread, FP32 pair arithmetic with compensated sums,
-//               reciprocal term against FP64-built per-bin phase factors (src/energy.jl:42-82);
+//   k_energy32  persistent CTAs of independent warps over (bin, 32-insertion tile) work items:
+//               each warp streams its bin's imaged neighbour list into its own shared-memory
+//               stages by bulk copies (cp.async.bulk + mbarrier, double buffered), one insertion
+//               per lane, FP32 pair arithmetic with a compensated sum, reciprocal term against
+//               FP64-built per-bin phase factors (src/energy.jl:42-82); in pa_energy32.cuh;
 //   k_energy64  the plain FP64 form of the reference algorithm (linear loop over every atom,
 //               one minimum image per atom), tiles per framework;
 //   k_segsum    per PA_SEGMENT-insertion segment: max, then Σ exp(x - max) and Σ ΔU exp(x - max),
@@ -30,6 +31,7 @@ template <> struct Vec4<double> { typedef double4 T; };
 template <typename F>
 struct DevBatch {
     int32_t nsys, nfw, ntypes, nguest, has_charge, nbins;
+    int32_t nsub;                                 // sub-bins per bin for the survivor ordering
     F rl2, re2;                                   // LJ and Ewald cutoffs squared
     const int32_t* framework_of;                  // nsys
     const F* cells;                               // 9*nfw column-major
@@ -80,7 +82,8 @@ struct Work {
     int32_t* slot;     // n_act
     int32_t* sorted;   // n_act: local insertion index in bin order
     double* dU;        // n_act: ΔU (+inf if rejected)
-    int32_t* bin_count;   // nbins
+    int32_t* bin_count;   // nbins*nsub: survivors per sub-bin
+    int32_t* fine_start;  // nbins*nsub+1
     int32_t* bin_start;   // nbins+1
     int32_t* tile_start;  // nbins+1
     int32_t* counters;    // [0] tile cursor, [1] total tiles, [2] error code, [3] survivors
@@ -196,13 +199,21 @@ __global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w
         w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
         return;
     }
+    // spatial bin of the pose's reference point; with nsub = 64, a 4x4x4 Z-ordered sub-bin
+    // inside it orders the survivors so that neighbouring threads hold nearby insertions
     const int32_t* nb = b.bin_dims + 3 * fw;
-    int32_t bx = min(int32_t(float(rp[0]) * float(nb[0])), nb[0] - 1);
-    int32_t by = min(int32_t(float(rp[1]) * float(nb[1])), nb[1] - 1);
-    int32_t bz = min(int32_t(float(rp[2]) * float(nb[2])), nb[2] - 1);
-    int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
-    w.bin_of[t] = bin;
-    w.slot[t] = atomicAdd(&w.bin_count[bin], 1);
+    const float fx = float(rp[0]) * float(nb[0]), fy = float(rp[1]) * float(nb[1]), fz = float(rp[2]) * float(nb[2]);
+    const int32_t bx = min(int32_t(fx), nb[0] - 1), by = min(int32_t(fy), nb[1] - 1), bz = min(int32_t(fz), nb[2] - 1);
+    const int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
+    int32_t sub = 0;
+    if (b.nsub == 64) {
+        const uint32_t sx = min(uint32_t((fx - float(bx)) * 4.f), 3u), sy = min(uint32_t((fy - float(by)) * 4.f), 3u),
+                       sz = min(uint32_t((fz - float(bz)) * 4.f), 3u);
+        sub = int32_t((sx & 1) | ((sy & 1) << 1) | ((sz & 1) << 2) | ((sx & 2) << 2) | ((sy & 2) << 3) | ((sz & 2) << 4));
+    }
+    const int32_t fine = bin * b.nsub + sub;
+    w.bin_of[t] = fine;
+    w.slot[t] = atomicAdd(&w.bin_count[fine], 1);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -234,24 +245,39 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* s_warp, i
     return warp_excl + x - v;
 }
 
-__global__ void __launch_bounds__(1024) k_scan(Work w, int32_t nbins, int32_t tile) {
+__global__ void __launch_bounds__(1024) k_scan(Work w, int32_t nbins, int32_t nsub, int32_t tile) {
     __shared__ int32_t s_warp[32];
-    int32_t carry_b = 0, carry_t = 0;
-    for (int32_t base = 0; base < nbins; base += blockDim.x) {
-        int32_t b = base + threadIdx.x;
-        int32_t c = b < nbins ? w.bin_count[b] : 0;
-        int32_t nt = (c + tile - 1) / tile;
-        int32_t tb, tt;
-        int32_t eb = block_excl_scan(c, s_warp, &tb);
-        int32_t et = block_excl_scan(nt, s_warp, &tt);
-        if (b < nbins) { w.bin_start[b] = carry_b + eb; w.tile_start[b] = carry_t + et; }
-        carry_b += tb; carry_t += tt;
+    const int32_t nfine = nbins * nsub;
+    int32_t carry = 0;
+    for (int32_t base = 0; base < nfine; base += blockDim.x) {  // survivors per sub-bin -> starts
+        const int32_t f = base + threadIdx.x;
+        const int32_t c = f < nfine ? w.bin_count[f] : 0;
+        int32_t tot;
+        const int32_t e = block_excl_scan(c, s_warp, &tot);
+        if (f < nfine) w.fine_start[f] = carry + e;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) w.fine_start[nfine] = carry;
+    __syncthreads();
+    int32_t carry_t = 0;
+    for (int32_t base = 0; base < nbins; base += blockDim.x) {  // tiles per bin
+        const int32_t bn = base + threadIdx.x;
+        int32_t nt = 0;
+        if (bn < nbins) {
+            const int32_t s0 = w.fine_start[bn * nsub], s1 = w.fine_start[(bn + 1) * nsub];
+            w.bin_start[bn] = s0;
+            nt = (s1 - s0 + tile - 1) / tile;
+        }
+        int32_t tt;
+        const int32_t et = block_excl_scan(nt, s_warp, &tt);
+        if (bn < nbins) w.tile_start[bn] = carry_t + et;
+        carry_t += tt;
     }
     if (threadIdx.x == 0) {
-        w.bin_start[nbins] = carry_b;
+        w.bin_start[nbins] = carry;
         w.tile_start[nbins] = carry_t;
         w.counters[1] = carry_t;
-        w.counters[3] = carry_b;
+        w.counters[3] = carry;
     }
 }
 
@@ -259,7 +285,7 @@ __global__ void k_scatter(Work w, int64_t n_act) {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= n_act) return;
     int32_t bin = w.bin_of[t];
-    if (bin >= 0) w.sorted[w.bin_start[bin] + w.slot[t]] = int32_t(t);
+    if (bin >= 0) w.sorted[w.fine_start[bin] + w.slot[t]] = int32_t(t);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -316,217 +342,7 @@ __device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
     return p * __expf(-z * z) * ri;
 }
 
-// ---------------------------------------------------------------------------------------------
-// k_energy32: persistent CTAs over (bin, tile) items; one insertion per thread.
-// ---------------------------------------------------------------------------------------------
-#define PA_TILE32 128
-#define PA_CHUNK32 512
-#define PA_KCHUNK 256
-#define PA_CTAS_PER_SM32 8
-
-template <int NS>
-__global__ void __launch_bounds__(PA_TILE32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
-    __shared__ __align__(128) float4 s_xyzq[2][PA_CHUNK32];
-    __shared__ __align__(128) int32_t s_type[2][PA_CHUNK32];
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ float2 s_B[PA_KCHUNK];
-    __shared__ float4 s_kc[PA_KCHUNK];
-    __shared__ int32_t s_item[4];
-    extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
-    const int tid = threadIdx.x;
-    const int nt = b.ntypes;
-    for (int x = tid; x < NS * nt; x += blockDim.x) { s_lj[x] = b.sig2[x]; s_lj[NS * nt + x] = b.eps4[x]; }
-    if (tid == 0) { mbar_init(&s_bar[0], 1); mbar_init(&s_bar[1], 1); mbar_fence_init(); }
-    __syncthreads();
-    const float* s_sig2 = s_lj;
-    const float* s_eps4 = s_lj + NS * nt;
-    uint32_t gchunk = 0;  // chunks consumed by this CTA so far (selects stage and parity)
-    const int32_t total_tiles = w.counters[1];
-    for (;;) {
-        if (tid == 0) {
-            int32_t t = atomicAdd(&w.counters[0], 1);
-            s_item[0] = t;
-            if (t < total_tiles) {
-                int32_t bin = find_bin(w.tile_start, b.nbins, t);
-                int32_t j0 = (t - w.tile_start[bin]) * PA_TILE32;
-                int32_t lo = w.bin_start[bin] + j0;
-                int32_t hi = min(lo + PA_TILE32, w.bin_start[bin + 1]);
-                s_item[1] = bin; s_item[2] = lo; s_item[3] = hi;
-            }
-        }
-        __syncthreads();
-        const int32_t t = s_item[0];
-        if (t >= total_tiles) break;
-        const int32_t bin = s_item[1], lo = s_item[2], hi = s_item[3];
-        __syncthreads();  // s_item may be overwritten at the next item
-        const int32_t fw = b.bin_fw[bin];
-        const int32_t l0 = b.list_offsets[bin], l1 = b.list_offsets[bin + 1];
-        const int32_t nch = (l1 - l0 + PA_CHUNK32 - 1) / PA_CHUNK32;
-        // prologue: first two chunks in flight
-        if (tid == 0) {
-            for (int c = 0; c < 2 && c < nch; ++c) {
-                uint32_t st = (gchunk + c) & 1;
-                int32_t e0 = l0 + c * PA_CHUNK32, n = min(PA_CHUNK32, l1 - e0);
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&s_bar[st], uint32_t(n) * 20u);
-                bulk_g2s(s_xyzq[st], b.list_xyzq + e0, uint32_t(n) * 16u, &s_bar[st]);
-                bulk_g2s(s_type[st], b.list_type + e0, uint32_t(n) * 4u, &s_bar[st]);
-            }
-        }
-        // this thread's insertion; a warp without one skips the arithmetic (it still takes part in
-        // the barriers and the shared-memory staging)
-        const bool active = lo + tid < hi;
-        const bool warp_live = __any_sync(0xffffffffu, active);
-        const int32_t li = active ? w.sorted[lo + tid] : 0;
-        const int32_t* nb = b.bin_dims + 3 * fw;
-        const int32_t lb = bin - b.bin_base[fw];
-        const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
-        const float cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
-        const float cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
-        const float cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
-        const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
-        const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
-        const float* A = b.cells + 9 * fw;
-        const float* iA = b.invcells + 9 * fw;
-        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
-        // site positions relative to the bin centre (Cartesian) and their fractional offsets
-        float px[NS], py[NS], pz[NS], dfr[3 * NS];
-        {
-            const float q[4] = {pq.x, pq.y, pq.z, pq.w};
-            float gsb[3 * NS];
-#pragma unroll
-            for (int x = 0; x < 3 * NS; ++x) gsb[x] = b.gsite[x];
-            const float c0 = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0));
-            const float c1 = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0));
-            const float c2 = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0));
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                float g[3];
-                rotate_s(q, gsb + 3 * s, g);
-                px[s] = c0 + g[0]; py[s] = c1 + g[1]; pz[s] = c2 + g[2];
-                dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
-                dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
-                dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
-            }
-        }
-        float gqs[NS], gqk[NS];  // site charges, and the same times the Coulomb constant
-#pragma unroll
-        for (int s = 0; s < NS; ++s) { gqs[s] = b.gq[s]; gqk[s] = float(KE * double(b.gq[s])); }
-        const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
-        const bool charged = b.has_charge != 0;
-        // real-space sum of LJ + KE q q erfc(alpha r)/r pair terms, compensated
-        float esum = 0.f, ecmp = 0.f;
-        // tmo_at: chunk whose bulk copy did not arrive in time (-1: none). After a timeout no
-        // further copies are issued and only the chunk already in flight is still waited for.
-        int32_t tmo_at = -1;
-        for (int32_t c = 0; c < nch; ++c) {
-            const uint32_t g = gchunk + c, st = g & 1, par = (g >> 1) & 1;
-            const bool issued = tmo_at < 0 || c == tmo_at + 1;
-            if (!issued) break;
-            const bool late = !mbar_wait_bounded(&s_bar[st], par);
-            const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
-            if (tmo_at < 0 && !late && warp_live) {
-#pragma unroll 2
-                for (int32_t j = 0; j < n; ++j) {
-                    const float4 at = s_xyzq[st][j];
-                    const int32_t ty = s_type[st][j];
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        if (r2 < rc2) {
-                            float e = 0.f;
-                            if (r2 < rl2) {
-                                const float x = s_sig2[s * nt + ty] * rcp_nr(r2);
-                                const float x3 = x * x * x;
-                                e = s_eps4[s * nt + ty] * (x3 * x3 - x3);
-                            }
-                            if (charged && r2 < re2) e = fmaf(gqk[s] * at.w, erfc_over_r(r2, alpha), e);
-                            kahan_add(esum, ecmp, e);
-                        }
-                    }
-                }
-            }
-            // every thread is done with stage st; a late copy anywhere stops the pipeline
-            if (__syncthreads_or(late) && tmo_at < 0) tmo_at = c;
-            if (tid == 0 && tmo_at < 0 && c + 2 < nch) {
-                int32_t e0 = l0 + (c + 2) * PA_CHUNK32, nn = min(PA_CHUNK32, l1 - e0);
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&s_bar[st], uint32_t(nn) * 20u);
-                bulk_g2s(s_xyzq[st], b.list_xyzq + e0, uint32_t(nn) * 16u, &s_bar[st]);
-                bulk_g2s(s_type[st], b.list_type + e0, uint32_t(nn) * 4u, &s_bar[st]);
-            }
-        }
-        gchunk += uint32_t(nch);
-        if (tmo_at >= 0) {
-            if (tid == 0) atomicExch(&w.counters[2], 1);
-            return;
-        }
-        // Reciprocal term: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c} built in
-        // FP64 per bin, G_k = Σ_s q_s e^{2 pi i n.d_s} with d_s the site's fractional offset from
-        // the bin centre. k-vectors run in rows of equal (n1, n2); along a row n3 advances by the
-        // framework's step, so e^{2 pi i n.d_s} is carried by one complex multiplication per
-        // k-vector and evaluated directly only at row starts.
-        double elr = 0.0;
-        if (charged) {
-            const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
-            float stc[NS], sts[NS], cr[NS], ci[NS];
-            {
-                const float kst = b.kstep[fw];
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
-                    cr[s] = 1.f; ci[s] = 0.f;
-                }
-            }
-            for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK) {
-                const int32_t kn = min(PA_KCHUNK, k1 - kb);
-                for (int32_t x = tid; x < kn; x += blockDim.x) {
-                    const int32_t kk = kb + x;
-                    const float4 kc = b.kcoef4[kk];
-                    s_kc[x] = kc;
-                    // phase of the bin centre in turns, reduced in FP64
-                    double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
-                    ph -= rint(ph);
-                    double sn, cs;
-                    sincospi(2.0 * ph, &sn, &cs);
-                    const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
-                    // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
-                    s_B[x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
-                }
-                __syncthreads();
-                if (warp_live) {
-                    float acc = 0.f, cacc = 0.f;
-                    for (int32_t x = 0; x < kn; ++x) {
-                        const float4 kc = s_kc[x];
-                        if (kc.w == 0.f) {  // row start: direct evaluation
-#pragma unroll
-                            for (int s = 0; s < NS; ++s) {
-                                const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
-                                sincospif(2.0f * ph, &ci[s], &cr[s]);
-                            }
-                        } else {  // next k-vector of the row
-#pragma unroll
-                            for (int s = 0; s < NS; ++s) {
-                                const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
-                                ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
-                                cr[s] = r;
-                            }
-                        }
-                        float gr = 0.f, gi = 0.f;
-#pragma unroll
-                        for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
-                        const float2 B = s_B[x];
-                        kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
-                    }
-                    elr += double(acc) - double(cacc);
-                }
-                __syncthreads();
-            }
-        }
-        if (active) w.dU[li] = double(esum) - double(ecmp) + KE * elr + b.const_offset[fw];
-    }
-}
+#include "pa_energy32.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // k_energy64: the plain FP64 form of the reference algorithm (src/energy.jl:42-82): for every
