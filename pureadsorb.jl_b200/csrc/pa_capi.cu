@@ -69,9 +69,10 @@ struct pa_batch {
     void* lists = nullptr;
     pa::DevBatch<float> d32{};
     pa::DevBatch<double> d64{};
+    // cudaFree returns stream-ordered pool memory synchronously, so the next upload reuses it
     ~pa_batch() {
-        if (arena) cudaFreeAsync(arena, 0);
-        if (lists) cudaFreeAsync(lists, 0);
+        if (arena) cudaFree(arena);
+        if (lists) cudaFree(lists);
     }
 };
 
@@ -216,7 +217,7 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     char* a = static_cast<char*>(B->arena);
     char* l = static_cast<char*>(B->lists);
     d.nsys = B->nsys; d.nfw = B->nfw; d.ntypes = B->ntypes; d.nguest = B->nguest; d.nbins = B->nbins;
-    d.nsub = sizeof(F) == 4 ? 64 : 1;
+    d.nsub = sizeof(F) == 4 ? 8 : 1;
     d.rl2 = F(desc->cutoff * desc->cutoff);
     d.re2 = F(desc->ewald_cutoff * desc->ewald_cutoff);
     d.framework_of = reinterpret_cast<const int32_t*>(a + o.framework_of);
@@ -359,7 +360,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.sig2 = pk.add(sig2);
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
     const bool lists = sizeof(F) == 4;
-    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0;
+    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0;
     if (lists) {
         std::vector<double> frac(3 * na), q(desc->charges, desc->charges + na);
         for (int fw = 0; fw < nfw; ++fw)
@@ -370,6 +371,15 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
                                       iA[r + 6] * desc->positions[3 * j + 2];
                 }
         std::vector<double> cells64(desc->cells, desc->cells + 9 * nfw);
+        // each framework's atoms in type-major order: list entries of one type form one run
+        std::vector<int32_t> order(na);
+        for (int fw = 0; fw < nfw; ++fw) {
+            const int32_t a0 = B->atom_offsets[fw], a1 = B->atom_offsets[fw + 1];
+            for (int32_t j = a0; j < a1; ++j) order[j] = j;
+            std::stable_sort(order.begin() + a0, order.begin() + a1,
+                             [&](int32_t x, int32_t y) { return types[x] < types[y]; });
+        }
+        t_order = pk.add(order);
         t_frac = pk.add(frac); t_q = pk.add(q); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
         t_nimg = pk.add(nimg); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
     }
@@ -382,6 +392,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         g.frac = reinterpret_cast<const double*>(base + t_frac); g.charges = reinterpret_cast<const double*>(base + t_q);
         g.types = reinterpret_cast<const int32_t*>(base + o.types); g.cells = reinterpret_cast<const double*>(base + t_cells);
         g.atom_offsets = reinterpret_cast<const int32_t*>(base + o.atom_offsets);
+        g.order = reinterpret_cast<const int32_t*>(base + t_order);
         g.bin_dims = reinterpret_cast<const int32_t*>(base + o.bin_dims);
         g.bin_base = reinterpret_cast<const int32_t*>(base + o.bin_base);
         g.bin_fw = reinterpret_cast<const int32_t*>(base + o.bin_fw);
@@ -442,10 +453,15 @@ cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::W
     if (B->precision == PA_PRECISION_F32) {
         size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
         if (dyn > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+            cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(pa::k_energy32<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
             if (e != cudaSuccess) return e;
         }
-        pa::k_energy32<NS><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+        if (B->d32.rl2 == B->d32.re2)
+            pa::k_energy32<NS, true><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+        else
+            pa::k_energy32<NS, false><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
@@ -633,7 +649,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     PA_CUDA(ctx, ctx->slot.ensure(sizeof(int32_t) * n_act));
     PA_CUDA(ctx, ctx->sorted.ensure(sizeof(int32_t) * n_act));
     PA_CUDA(ctx, ctx->dU.ensure(sizeof(double) * n_act));
-    const int32_t nsub = f32 ? 64 : 1;
+    const int32_t nsub = f32 ? 8 : 1;
     const int64_t nfine = int64_t(B->nbins) * nsub;
     if (nfine + 1 > INT32_MAX) return fail(ctx, PA_ERR_ARG, "too many spatial bins");
     PA_CUDA(ctx, ctx->bin_count.ensure(sizeof(int32_t) * (nfine + 1)));

@@ -16,7 +16,19 @@
 #define PA_KCHUNK32 64
 #define PA_CTAS_PER_SM32 8
 
-template <int NS>
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms.
+template <int NS, bool EQCUT>
 __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(128) int32_t s_type[PA_WARPS32][2][PA_CHUNK32];
@@ -103,6 +115,13 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         }
         const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
         float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
+        // LJ parameters of the current type for each site: list entries come in runs of one type,
+        // and the type is the same for every lane, so the reload is a uniform branch
+        int32_t cur = -1;
+        float sg[NS], ep[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) { sg[s] = 0.f; ep[s] = 0.f; }
+        const float NLOG2E = -1.4426950408889634f;
         // tmo_at: chunk whose copy did not arrive in time (-1: none); after it no copies are issued
         // and only the chunk already in flight is still waited for
         int32_t tmo_at = -1;
@@ -117,6 +136,11 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                 for (int32_t j = 0; j < n; ++j) {
                     const float4 at = xyzq[st][j];
                     const int32_t ty = typ[st][j];
+                    if (ty != cur) {
+                        cur = ty;
+#pragma unroll
+                        for (int s = 0; s < NS; ++s) { sg[s] = s_sig2[s * nt + ty]; ep[s] = s_eps4[s * nt + ty]; }
+                    }
 #pragma unroll
                     for (int s = 0; s < NS; ++s) {
                         const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
@@ -125,26 +149,26 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                             float e = 0.f;
                             if (charged) {
                                 // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
-                                float ri = rsqrtf(r2);
+                                float ri = rsqrt_ftz(r2);
                                 ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
-                                if (r2 < rl2) {
-                                    const float x = s_sig2[s * nt + ty] * (ri * ri);
+                                if (EQCUT || r2 < rl2) {
+                                    const float x = sg[s] * (ri * ri);
                                     const float x3 = x * x * x;
-                                    e = s_eps4[s * nt + ty] * (x3 * x3 - x3);
+                                    e = ep[s] * (x3 * x3 - x3);
                                 }
-                                if (r2 < re2) {
+                                if (EQCUT || r2 < re2) {
                                     const float z = alpha * (r2 * ri);
                                     const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
                                     const float cf[PA_NERFC32] = PA_ERFC32_INIT;
                                     float p = cf[PA_NERFC32 - 1];
 #pragma unroll
                                     for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
-                                    e = fmaf(gqk[s] * at.w, p * __expf(-z * z) * ri, e);
+                                    e = fmaf(gqk[s] * at.w, p * ex2_ftz((z * z) * NLOG2E) * ri, e);
                                 }
                             } else {
-                                const float x = s_sig2[s * nt + ty] * rcp_nr(r2);
+                                const float x = sg[s] * rcp_nr(r2);
                                 const float x3 = x * x * x;
-                                e = s_eps4[s * nt + ty] * (x3 * x3 - x3);
+                                e = ep[s] * (x3 * x3 - x3);
                             }
                             kahan_add(esum, ecmp, e);
                         }

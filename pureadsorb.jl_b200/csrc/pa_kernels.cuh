@@ -199,18 +199,15 @@ __global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w
         w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
         return;
     }
-    // spatial bin of the pose's reference point; with nsub = 64, a 4x4x4 Z-ordered sub-bin
-    // inside it orders the survivors so that neighbouring threads hold nearby insertions
+    // spatial bin of the pose's reference point; with nsub = 8 the octant inside it orders the
+    // survivors, so that a warp's 32 insertions lie in two adjacent octants
     const int32_t* nb = b.bin_dims + 3 * fw;
     const float fx = float(rp[0]) * float(nb[0]), fy = float(rp[1]) * float(nb[1]), fz = float(rp[2]) * float(nb[2]);
     const int32_t bx = min(int32_t(fx), nb[0] - 1), by = min(int32_t(fy), nb[1] - 1), bz = min(int32_t(fz), nb[2] - 1);
     const int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
     int32_t sub = 0;
-    if (b.nsub == 64) {
-        const uint32_t sx = min(uint32_t((fx - float(bx)) * 4.f), 3u), sy = min(uint32_t((fy - float(by)) * 4.f), 3u),
-                       sz = min(uint32_t((fz - float(bz)) * 4.f), 3u);
-        sub = int32_t((sx & 1) | ((sy & 1) << 1) | ((sz & 1) << 2) | ((sx & 2) << 2) | ((sy & 2) << 3) | ((sz & 2) << 4));
-    }
+    if (b.nsub == 8)
+        sub = int32_t(fx - float(bx) >= 0.5f) | (int32_t(fy - float(by) >= 0.5f) << 1) | (int32_t(fz - float(bz) >= 0.5f) << 2);
     const int32_t fine = bin * b.nsub + sub;
     w.bin_of[t] = fine;
     w.slot[t] = atomicAdd(&w.bin_count[fine], 1);
@@ -504,8 +501,9 @@ __global__ void __launch_bounds__(256) k_segsum(Work w, double kT) {
 // ---------------------------------------------------------------------------------------------
 // Neighbour lists of the FP32 path: for bin centre c (fractional, FP32-defined) and atom j with
 // fractional position f_j, every image A (f_j - c - round(f_j - c) + n), n in [-m, m]^3, within
-// radius R is one entry, stored relative to the bin centre. Order: atom index, then n (x fastest),
-// so the lists (and every energy sum over them) are deterministic. One CTA per bin.
+// radius R is one entry, stored relative to the bin centre. Order: atoms by type (then by index),
+// then n (x fastest), so the lists (and every energy sum over them) are deterministic and each
+// type is one contiguous run. One CTA per bin.
 // ---------------------------------------------------------------------------------------------
 struct ListGeom {
     const double* frac;        // 3*natoms fractional coordinates (cell-sorted order)
@@ -513,6 +511,7 @@ struct ListGeom {
     const int32_t* types;      // natoms, 0-based
     const double* cells;       // 9*nfw
     const int32_t* atom_offsets;
+    const int32_t* order;      // natoms: the framework's atoms ordered by type (stable), global indices
     const int32_t* bin_dims;   // 3*nfw
     const int32_t* bin_base;   // nfw+1
     const int32_t* bin_fw;     // nbins
@@ -549,7 +548,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         double dx = 0, dy = 0, dz = 0;
         int32_t j = 0;
         if (p < npairs) {
-            j = a0 + int32_t(p / nimgs);
+            j = g.order[a0 + int32_t(p / nimgs)];
             const int32_t im = int32_t(p % nimgs);
             const int32_t n0 = im % side - m, n1 = (im / side) % side - m, n2 = im / (side * side) - m;
             double d0 = St<double>::sub(g.frac[3 * j], c[0]), d1 = St<double>::sub(g.frac[3 * j + 1], c[1]),
