@@ -346,8 +346,10 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             }
         double R = rcmax + rg + circ + 1.0e-3;
         radius2[fw] = R * R;
+        // an image n of a fractional offset d in [-1/2, 1/2]^3 lies within R only if
+        // |d_r + n_r| <= R / L_r on every axis, so |n_r| <= floor(R / L_r + 1/2)
         double Lmin = std::min(L[0], std::min(L[1], L[2]));
-        nimg[fw] = int32_t(std::ceil(R / Lmin + 0.5));
+        nimg[fw] = int32_t(std::floor(R / Lmin + 0.5));
     }
     B->nbins = bbase[nfw];
     // one packed upload of every table (and the list build's temporaries)
@@ -416,13 +418,14 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             loff[q2 + 1] = loff[q2] + int32_t(padded);
         }
         B->list_entries = loff[B->nbins];
-        Packer lp;
-        o.list_offsets = lp.add(loff);
-        o.list_xyzq = lp.reserve(sizeof(float4) * size_t(std::max<int64_t>(1, B->list_entries)));
-        o.list_type = lp.reserve(sizeof(int32_t) * size_t(std::max<int64_t>(1, B->list_entries)));
-        PA_CUDA(ctx, cudaMallocAsync(&B->lists, lp.host.size(), st));
-        // only the offsets need the host copy; the entries are written by the fill pass
-        PA_CUDA(ctx, cudaMemcpyAsync(B->lists, lp.host.data(), o.list_xyzq, cudaMemcpyHostToDevice, st));
+        // one allocation: offsets, then the entries (written by the fill pass, never staged)
+        const auto up256 = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const size_t nent = size_t(std::max<int64_t>(1, B->list_entries));
+        o.list_offsets = 0;
+        o.list_xyzq = up256(sizeof(int32_t) * loff.size());
+        o.list_type = up256(o.list_xyzq + sizeof(float4) * nent);
+        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_type + sizeof(int32_t) * nent, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(B->lists, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st));
         char* lb = static_cast<char*>(B->lists);
         g.offsets = reinterpret_cast<const int32_t*>(lb + o.list_offsets);
         g.xyzq = reinterpret_cast<float4*>(lb + o.list_xyzq);
