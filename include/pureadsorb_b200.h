@@ -166,6 +166,19 @@ typedef struct pa_insertion_out {
 pa_status pa_widom(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
                    pa_insertion_out* per_insertion);
 
+/* Allocation-free variant of pa_widom; no counterpart in the reference. For callers that may
+ * not allocate device memory during the call (a host application that owns a fixed memory
+ * budget, strict per-tenant accounting, or code that must avoid cudaMalloc's device-wide
+ * synchronisation): the same kernels as pa_widom, with every per-call scratch buffer carved out
+ * of one file-scope device array of 16 MiB that each GPU loading the library holds until the
+ * process exits. Limits: at most 131,072 insertions per call, 1,024 systems, 32,768 spatial bins
+ * and 65,536 rejection radii; larger calls return PA_ERR_ARG. Only per_insertion->dU may be
+ * requested. All calls share the array (host calls are serialised by a mutex); device work of two
+ * calls must not overlap. The first call on a device looks up the array's address and should
+ * come before any stream capture. */
+pa_status pa_widom_static(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
+                          pa_insertion_out* per_insertion);
+
 /* Host-side pose of insertion k of system s (the same stream as the device), for callers that
  * need the poses without a GPU (e.g. the self-term orientations of FrameworkBatch). precision
  * selects 32- or 64-bit draws; rpos gets 3 and quat 4 values widened to FP64. */

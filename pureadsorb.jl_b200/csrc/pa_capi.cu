@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -815,3 +816,193 @@ pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, con
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free widom: pa_widom_static.
+//
+// Some callers cannot allocate device memory while they run: a host application that owns a
+// fixed device-memory budget and forbids plug-ins from touching the allocator, a service with
+// strict per-tenant memory accounting, or code that must not call cudaMalloc at all (which
+// synchronises the device). For them this entry point runs the same kernels as pa_widom with
+// every per-call scratch buffer carved out of one file-scope device array, so the call itself
+// allocates nothing on the device or the host heap. The batch (inputs) must already be uploaded
+// and the caller provides the outputs.
+//
+// The array is part of the library's device module: every GPU that loads the library holds its
+// PA_STATIC_SCRATCH_BYTES until the process exits. All calls share it and it keeps the last
+// call's contents, so each call clears what must start at zero; calls whose device work overlaps
+// (two host threads, or two streams) would race on it. Host calls are serialised by a mutex, but
+// a caller that mixes several contexts on one device must not let their device work overlap.
+// The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
+// that first call before any stream capture begins.
+// =============================================================================================
+namespace {
+
+constexpr int64_t ST_MAX_INSERT = 131072;         // insertions per call
+constexpr int64_t ST_MAX_BINS = 32768;            // spatial bins of the batch
+constexpr int64_t ST_MAX_FINE = ST_MAX_BINS * 8;  // sub-bins
+constexpr int64_t ST_MAX_SEG = 2048;              // PA_SEGMENT-insertion segments per call
+constexpr int64_t ST_MAX_SYS = 1024;              // systems
+constexpr int64_t ST_MAX_RHO2 = 65536;            // nsys * N * ntypes rejection radii
+constexpr size_t st_up(size_t x) { return (x + 255) & ~size_t(255); }
+// layout (byte offsets); the small per-call inputs come first so one copy uploads them
+constexpr size_t ST_SYS_OFF = 0;
+constexpr size_t ST_SEG_RNG = st_up(ST_SYS_OFF + 8 * (ST_MAX_SYS + 1));
+constexpr size_t ST_REACH0 = st_up(ST_SEG_RNG + 16 * ST_MAX_SEG);
+constexpr size_t ST_RHO2 = st_up(ST_REACH0 + 12 * ST_MAX_SYS);
+constexpr size_t ST_INPUT_END = st_up(ST_RHO2 + 8 * ST_MAX_RHO2);
+constexpr size_t ST_COUNTERS = ST_INPUT_END;
+constexpr size_t ST_BIN_COUNT = st_up(ST_COUNTERS + 4 * 8);
+constexpr size_t ST_FINE_START = st_up(ST_BIN_COUNT + 4 * (ST_MAX_FINE + 1));
+constexpr size_t ST_BIN_START = st_up(ST_FINE_START + 4 * (ST_MAX_FINE + 1));
+constexpr size_t ST_TILE_START = st_up(ST_BIN_START + 4 * (ST_MAX_BINS + 1));
+constexpr size_t ST_SEG_OUT = st_up(ST_TILE_START + 4 * (ST_MAX_BINS + 1));
+constexpr size_t ST_POSE_A = st_up(ST_SEG_OUT + 24 * ST_MAX_SEG);
+constexpr size_t ST_POSE_B = st_up(ST_POSE_A + 32 * ST_MAX_INSERT);
+constexpr size_t ST_BIN_OF = st_up(ST_POSE_B + 32 * ST_MAX_INSERT);
+constexpr size_t ST_SLOT = st_up(ST_BIN_OF + 4 * ST_MAX_INSERT);
+constexpr size_t ST_SORTED = st_up(ST_SLOT + 4 * ST_MAX_INSERT);
+constexpr size_t ST_DU = st_up(ST_SORTED + 4 * ST_MAX_INSERT);
+constexpr size_t ST_END = st_up(ST_DU + 8 * ST_MAX_INSERT);
+
+}  // namespace
+
+#define PA_STATIC_SCRATCH_BYTES (16u << 20)
+static_assert(ST_END <= PA_STATIC_SCRATCH_BYTES, "static scratch layout exceeds the array");
+
+static __device__ __align__(256) unsigned char pa_static_scratch[PA_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex st_mutex;                 // serialises host calls: the scratch and staging are shared
+void* st_addr[64] = {nullptr};       // device address of pa_static_scratch, per device
+unsigned char st_stage[ST_INPUT_END];  // host staging of the small per-call inputs
+int64_t st_ns[ST_MAX_SYS];
+Seg st_segs[ST_MAX_SEG];
+double st_segout[3 * ST_MAX_SEG];
+int32_t st_counters[8];
+
+}  // namespace
+
+extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const pa_widom_args* args,
+                                     pa_block_sums* sums, pa_insertion_out* per) {
+    if (!ctx || !B || !args || !sums) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
+    if (!sums->lse_max || !sums->sum_w || !sums->sum_uw || !sums->count) return fail(ctx, PA_ERR_ARG, "null block-sum array");
+    if (per && (per->flags || per->poses))
+        return fail(ctx, PA_ERR_ARG, "pa_widom_static returns per-insertion dU only (flags and poses need host staging)");
+    const int64_t ninsert = args->ninsert, nblocks = args->nblocks, run = args->run;
+    if (ninsert < 1 || nblocks < 1 || run < 1) return fail(ctx, PA_ERR_ARG, "ninsert, nblocks and run must be >= 1");
+    if (!(std::isfinite(args->kT) && args->kT != 0)) return fail(ctx, PA_ERR_ARG, "kT must be finite and nonzero");
+    if (args->reject && (!args->rho2 || !args->reach0)) return fail(ctx, PA_ERR_ARG, "reject needs rho2 and reach0");
+    const int nsys = B->nsys, N = B->nguest, nt = B->ntypes;
+    const bool f32 = B->precision == PA_PRECISION_F32;
+    const int32_t nsub = f32 ? 8 : 1;
+    if (ninsert > ST_MAX_INSERT)
+        return fail(ctx, PA_ERR_ARG, "pa_widom_static: ninsert=" + std::to_string(ninsert) + " exceeds its maximum of " +
+                                         std::to_string(ST_MAX_INSERT) + " insertions per call");
+    if (nsys > ST_MAX_SYS || int64_t(B->nbins) > ST_MAX_BINS || int64_t(nsys) * N * nt > ST_MAX_RHO2)
+        return fail(ctx, PA_ERR_ARG, "pa_widom_static: batch exceeds the static scratch limits (" +
+                                         std::to_string(ST_MAX_SYS) + " systems, " + std::to_string(ST_MAX_BINS) +
+                                         " spatial bins, " + std::to_string(ST_MAX_RHO2) + " rejection radii)");
+    std::lock_guard<std::mutex> lock(st_mutex);
+    // per-system counts and segments, in fixed host storage
+    {
+        int64_t q = ninsert / run, rem = ninsert % run, full = q / nsys, hi = q % nsys;
+        for (int s = 0; s < nsys; ++s) st_ns[s] = full * run + (s < hi ? run : 0);
+        if (rem > 0) st_ns[q % nsys] += rem;
+    }
+    int64_t* off = reinterpret_cast<int64_t*>(st_stage + ST_SYS_OFF);
+    off[0] = 0;
+    for (int s = 0; s < nsys; ++s) {
+        if (st_ns[s] < nblocks) return fail(ctx, PA_ERR_ARG, "system " + std::to_string(s + 1) + " gets fewer samples than nblocks");
+        off[s + 1] = off[s] + st_ns[s];
+    }
+    int64_t nseg_all = 0;
+    for (int s = 0; s < nsys; ++s) {
+        const int64_t blen = st_ns[s] / nblocks;
+        for (int64_t b = 0; b < nblocks; ++b) {
+            const int64_t k0 = b * blen, k1 = (b == nblocks - 1) ? st_ns[s] : (b + 1) * blen;
+            for (int64_t k = k0; k < k1; k += PA_SEGMENT) {
+                if (nseg_all >= ST_MAX_SEG)
+                    return fail(ctx, PA_ERR_ARG, "pa_widom_static: more than " + std::to_string(ST_MAX_SEG) + " segments");
+                st_segs[nseg_all++] = Seg{int64_t(s), b, off[s] + k, off[s] + std::min<int64_t>(k + PA_SEGMENT, k1)};
+            }
+        }
+    }
+    for (int64_t q = 0; q < int64_t(nsys) * nblocks; ++q) {
+        sums->lse_max[q] = -INFINITY; sums->sum_w[q] = 0; sums->sum_uw[q] = 0; sums->count[q] = 0;
+    }
+    const int64_t sb = std::max<int64_t>(0, args->segment_begin);
+    const int64_t se = args->segment_end <= 0 ? nseg_all : std::min(args->segment_end, nseg_all);
+    if (sb >= se) return PA_OK;
+    const int64_t i_lo = st_segs[sb].i0, n_act = st_segs[se - 1].i1 - i_lo, nseg = se - sb;
+    int64_t* rng = reinterpret_cast<int64_t*>(st_stage + ST_SEG_RNG);
+    for (int64_t q = 0; q < nseg; ++q) { rng[2 * q] = st_segs[sb + q].i0 - i_lo; rng[2 * q + 1] = st_segs[sb + q].i1 - i_lo; }
+    if (args->reject) {
+        std::memcpy(st_stage + ST_REACH0, args->reach0, sizeof(int32_t) * 3 * nsys);
+        const int64_t nr = int64_t(nsys) * N * nt;
+        if (f32) {
+            float* r2 = reinterpret_cast<float*>(st_stage + ST_RHO2);
+            for (int64_t q = 0; q < nr; ++q) r2[q] = float(args->rho2[q]);
+        } else {
+            std::memcpy(st_stage + ST_RHO2, args->rho2, sizeof(double) * nr);
+        }
+    }
+    if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, PA_ERR_ARG, "device index out of range");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    if (!st_addr[ctx->device]) {  // once per device, with that device current
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, pa_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(ctx, PA_ERR_CUDA, std::string("cudaGetSymbolAddress(pa_static_scratch): ") + cudaGetErrorString(e));
+        st_addr[ctx->device] = p;
+    }
+    char* base = static_cast<char*>(st_addr[ctx->device]);
+    cudaStream_t st = ctx->stream;
+    PA_CUDA(ctx, cudaMemcpyAsync(base, st_stage, ST_INPUT_END, cudaMemcpyHostToDevice, st));
+    const int64_t nfine = int64_t(B->nbins) * nsub;
+    PA_CUDA(ctx, cudaMemsetAsync(base + ST_BIN_COUNT, 0, sizeof(int32_t) * (nfine + 1), st));
+    PA_CUDA(ctx, cudaMemsetAsync(base + ST_COUNTERS, 0, sizeof(int32_t) * 8, st));
+    pa::Work w{};
+    if (f32) { w.pose_a = reinterpret_cast<float4*>(base + ST_POSE_A); w.pose_b = reinterpret_cast<float4*>(base + ST_POSE_B); }
+    else { w.pose64a = reinterpret_cast<double4*>(base + ST_POSE_A); w.pose64b = reinterpret_cast<double4*>(base + ST_POSE_B); }
+    w.bin_of = reinterpret_cast<int32_t*>(base + ST_BIN_OF); w.slot = reinterpret_cast<int32_t*>(base + ST_SLOT);
+    w.sorted = reinterpret_cast<int32_t*>(base + ST_SORTED); w.dU = reinterpret_cast<double*>(base + ST_DU);
+    w.bin_count = reinterpret_cast<int32_t*>(base + ST_BIN_COUNT); w.fine_start = reinterpret_cast<int32_t*>(base + ST_FINE_START);
+    w.bin_start = reinterpret_cast<int32_t*>(base + ST_BIN_START); w.tile_start = reinterpret_cast<int32_t*>(base + ST_TILE_START);
+    w.counters = reinterpret_cast<int32_t*>(base + ST_COUNTERS); w.seg_out = reinterpret_cast<double*>(base + ST_SEG_OUT);
+    w.seg_rng = reinterpret_cast<const int64_t*>(base + ST_SEG_RNG);
+    pa::CallArgs ca{};
+    ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = reinterpret_cast<const int64_t*>(base + ST_SYS_OFF);
+    ca.seed = args->seed; ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
+    const int32_t* reach0 = reinterpret_cast<const int32_t*>(base + ST_REACH0);
+    if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, reinterpret_cast<const float*>(base + ST_RHO2), reach0, st))); }
+    else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, reinterpret_cast<const double*>(base + ST_RHO2), reach0, st))); }
+    PA_CUDA(ctx, cudaGetLastError());
+    pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
+    pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
+    PA_CUDA(ctx, cudaGetLastError());
+    {
+        cudaError_t e = cudaSuccess;
+        PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, st)));
+        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+    }
+    pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT);
+    PA_CUDA(ctx, cudaGetLastError());
+    PA_CUDA(ctx, cudaMemcpyAsync(st_segout, base + ST_SEG_OUT, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(st_counters, base + ST_COUNTERS, sizeof(st_counters), cudaMemcpyDeviceToHost, st));
+    if (per && per->dU)
+        PA_CUDA(ctx, cudaMemcpyAsync(per->dU + i_lo, base + ST_DU, sizeof(double) * n_act, cudaMemcpyDeviceToHost, st));
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    if (st_counters[2] != 0) return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
+    if (sums->segments)
+        for (int64_t q = 0; q < nseg; ++q)
+            for (int r = 0; r < 3; ++r) sums->segments[3 * (sb + q) + r] = st_segout[3 * q + r];
+    for (int64_t q = 0; q < nseg; ++q) {
+        const Seg& g = st_segs[sb + q];
+        combine_segment(sums, g.s * nblocks + g.b, g.i1 - g.i0, st_segout + 3 * q);
+    }
+    return PA_OK;
+}
