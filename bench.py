@@ -14,7 +14,6 @@ import argparse
 import json
 import math
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -27,6 +26,9 @@ import __graft_entry__ as ge  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
+# DRAM bytes (read + write) of one k_energy32 launch on this workload, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
+ENERGY32_TRAFFIC_BYTES = 101.298688e6 + 4.943616e6
 
 
 def parse():
@@ -42,54 +44,50 @@ def parse():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled through NVML (read-only) every 5 ms during the timed
+    region; falls back to nvidia-smi when NVML is unavailable."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
     def __init__(self, device):
         self.device = device
-        self.samples = []
-        self.proc = None
+        self.samples = []  # (sm MHz, reason bits)
+        self.max_mhz = None
+        self.stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM),
+                                             pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
             self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+        except Exception:
+            self.thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                self.samples.append(f)
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.thread:
+            self.thread.join(timeout=2)
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        reasons = set()
-        for s in self.samples:
-            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), s[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        reasons = sorted({name for _, bits in self.samples for bit, name in self.REASONS.items() if bits & bit})
+        return {"sm_mhz": float(np.median([m for m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples)}
 
 
 def load_peaks():
@@ -256,7 +254,8 @@ def main():
         peak = fp32_peak(torch)
         ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
+                "traffic": ENERGY32_TRAFFIC_BYTES if args.ninsert == 1_000_000 and world == 1 else None,
+                "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
                 "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
                 "flops_per_survivor": flops_surv, "reference_algorithm_flops_per_survivor": ref_alg,
                 "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew}
