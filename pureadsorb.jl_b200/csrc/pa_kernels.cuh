@@ -152,15 +152,21 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
         stencil_start_count(h2, m2, n2, &st2, &c2);
         stencil_start_count(h3, m3, n3, &st3, &c3);
         const F* r2a = r2row + a * nt;
+        // The x-cells of one (y, z) row of the stencil are consecutive in the cell-sorted atom
+        // array, so each row is one contiguous atom range, or two where it wraps around the grid.
+        // Atoms are visited in the same order as cell by cell (x innermost).
+        const int32_t xa0 = st1 < 0 ? st1 + n1 : st1;
+        const int32_t xa1 = st1 < 0 ? n1 : min(st1 + c1, n1);
+        const int32_t xb1 = st1 < 0 ? st1 + c1 : max(st1 + c1 - n1, 0);
         for (int32_t t3 = 0; t3 < c3; ++t3) {
-            int32_t z = wrap_cell(st3 + t3, n3);
+            const int32_t z = wrap_cell(st3 + t3, n3);
             for (int32_t t2 = 0; t2 < c2; ++t2) {
-                int32_t y = wrap_cell(st2 + t2, n2);
-                for (int32_t t1 = 0; t1 < c1; ++t1) {
-                    int32_t x = wrap_cell(st1 + t1, n1);
-                    int32_t c = x + n1 * (y + n2 * z);
-                    int32_t j1 = a0 + coff[c + 1];
-                    for (int32_t j = a0 + coff[c]; j < j1; ++j) {
+                const int32_t row = n1 * (wrap_cell(st2 + t2, n2) + n2 * z);
+                // part A: cells [xa0, xa1); part B (wrapped): cells [0, xb1)
+                for (int part = 0; part < 2; ++part) {
+                    const int32_t j0 = a0 + coff[row + (part == 0 ? xa0 : 0)];
+                    const int32_t j1 = a0 + coff[row + (part == 0 ? xa1 : xb1)];
+                    for (int32_t j = j0; j < j1; ++j) {
                         typename Vec4<F>::T at = b.atoms[j];
                         F D[3] = {S::sub(sp[0], at.x), S::sub(sp[1], at.y), S::sub(sp[2], at.z)};
                         minimum_image_s(Ael, iAel, D);
