@@ -166,6 +166,14 @@ typedef struct pa_insertion_out {
 pa_status pa_widom(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
                    pa_insertion_out* per_insertion);
 
+/* Rejection radii and phase-0 stencil reaches of one widom call, on the host
+ * (`build_rejection_tables`, src/widom.jl:202-253): rho2 gets nsys*N*nt values, reach0 3*nsys.
+ * bs and kmin are the batch's `bs` (nfw) and `kmin` (nfw*N*nt); eps_F is eps of the batch's
+ * float type. Returns PA_ERR_ARG (and the 1-based system in *bad_system) when a system's margin
+ * is not positive or a root search fails. Needs no device. */
+pa_status pa_rejection_tables(const pa_batch_desc* desc, const double* bs, const double* kmin, double kT, double eps_F,
+                              double* rho2, int32_t* reach0, int32_t* bad_system);
+
 /* Allocation-free variant of pa_widom; no counterpart in the reference. For callers that may
  * not allocate device memory during the call (a host application that owns a fixed memory
  * budget, strict per-tenant accounting, or code that must avoid cudaMalloc's device-wide

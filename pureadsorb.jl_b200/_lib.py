@@ -68,6 +68,7 @@ SIGNATURES = [
     ("pa_batch_info", _i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     ("pa_widom", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
     ("pa_widom_static", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
+    ("pa_rejection_tables", _i32, [ctypes.POINTER(BatchDesc), _p, _p, _f64, _f64, _p, _p, ctypes.POINTER(_i32)]),
     ("pa_segment_count", _i32, [_i64, _i32, _i32, _i32, ctypes.POINTER(_i64)]),
     ("pa_combine_segments", _i32, [_i64, _i32, _i32, _i32, _p, ctypes.POINTER(BlockSums)]),
     ("pa_pose_host", _i32, [_i32, _u64, _u64, _u64, _p, _p]),

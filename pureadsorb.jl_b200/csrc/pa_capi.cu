@@ -1006,3 +1006,77 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     }
     return PA_OK;
 }
+
+// =============================================================================================
+// Host: rejection radii and phase-0 stencil reaches of one call (build_rejection_tables,
+// src/widom.jl:202-253; find_rho2, src/reject.jl:168-209; theta_F, src/reject.jl:11-19).
+// =============================================================================================
+namespace {
+
+double theta_f64() {
+    static double theta = [] {
+        double lo = 0, hi = 2000;
+        while (std::nextafter(lo, hi) != hi) {
+            double mid = lo + (hi - lo) / 2;
+            if (std::exp(-mid) == 0.0) hi = mid; else lo = mid;
+        }
+        return hi;
+    }();
+    return theta;
+}
+
+inline double lj4(double r2, double s, double e) { double x = s * s / r2; x = x * x * x; return 4 * e * (x * x - x); }
+
+// first root of LJ(r) - |kmin|/r = margin scanning up from r -> 0, clamped to r_lj; 0 for an
+// infinite margin or a zero epsilon; -1 when a search exceeds its iteration cap
+double rho2_of(double s, double e, double kmin, double margin, double r_lj) {
+    if (std::isinf(margin) || e == 0) return 0;
+    auto f = [&](double r) { return lj4(r * r, s, e) - std::fabs(kmin) / r - margin; };
+    const int cap = 200;
+    const double eps = 2.220446049250313e-16;
+    double hi = s; int it = 0;
+    while (f(hi) >= 0) { hi *= 2; if (++it > cap) return -1; }
+    double lo = hi; it = 0;
+    while (f(lo) < 0) { lo /= 2; if (++it > cap) return -1; }
+    it = 0;
+    while (hi - lo > 4 * eps * hi) {
+        double mid = (lo + hi) / 2;
+        if (f(mid) > 0) lo = mid; else hi = mid;
+        if (++it > cap) return -1;
+    }
+    double r = std::min((lo + hi) / 2, r_lj);
+    return r * r;
+}
+
+}  // namespace
+
+extern "C" pa_status pa_rejection_tables(const pa_batch_desc* d, const double* bs, const double* kmin, double kT,
+                                         double eps_F, double* rho2, int32_t* reach0, int32_t* bad_system) {
+    if (!d || !bs || !kmin || !rho2 || !reach0) return PA_ERR_ARG;
+    if (bad_system) *bad_system = 0;
+    const int N = d->nguest, nt = d->ntypes;
+    const double theta = theta_f64();
+    for (int s = 0; s < d->nsys; ++s) {
+        const int fw = d->framework_of[s] - 1;
+        const double Bs = bs[fw], cs = d->constant_offset[fw];
+        const double natoms = d->atom_offsets[fw + 1] - d->atom_offsets[fw], nk = d->k_offsets[fw + 1] - d->k_offsets[fw];
+        const double n = N * natoms + nk + 8;
+        const double safety = 2 * n * eps_F * (Bs + std::fabs(cs)) + 4.0e-6 * Bs;
+        const double margin = std::isinf(Bs) ? INFINITY : (theta + 2) * kT + safety + Bs - cs;
+        if (!(margin > 0)) { if (bad_system) *bad_system = s + 1; return PA_ERR_ARG; }
+        double rmax = 0;
+        for (int a = 0; a < N; ++a)
+            for (int t = 0; t < nt; ++t) {
+                const int gt = d->guest_types[a] - 1;
+                const double r2 = rho2_of(d->sigma[gt + nt * t], d->epsilon[gt + nt * t],
+                                          kmin[int64_t(fw) * N * nt + a * nt + t], margin, d->cutoff);
+                if (r2 < 0) { if (bad_system) *bad_system = s + 1; return PA_ERR_ARG; }
+                rho2[int64_t(s) * N * nt + a * nt + t] = r2;
+                rmax = std::max(rmax, r2);
+            }
+        double L[3];
+        perpendicular_lengths(d->cells + 9 * fw, L);
+        for (int r = 0; r < 3; ++r) reach0[3 * s + r] = int32_t(std::ceil(std::sqrt(rmax) * d->ncells[3 * fw + r] / L[r]));
+    }
+    return PA_OK;
+}

@@ -9,10 +9,9 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from .cell import perpendicular_lengths, stencil_reaches
 from .constants import KB
 from .errors import ArgumentError
-from .reject import find_rho2, theta_F
+from .reject import theta_F
 
 
 @dataclass(frozen=True)
@@ -61,39 +60,24 @@ def boltzmann_weight(dU, kT):
 
 def build_rejection_tables(batch, kT):
     """Rejection radii rho2 (nsys*N*ntypes) and phase-0 stencil half-widths reach0 (nsys x 3) for
-    one call (src/widom.jl:202-253). The summation-error term uses eps of the batch's float type;
-    theta is theta_F(Float64) because weights accumulate in FP64."""
+    one call (src/widom.jl:202-253), computed by the library's host code (pa_rejection_tables).
+    The summation-error term uses eps of the batch's float type; theta is theta_F(Float64)
+    because weights accumulate in FP64."""
     N = len(batch.guest_types)
     nt = len(batch.sigma)
-    eps_F = float(np.finfo(batch.T).eps)
-    theta = float(theta_F(np.float64))
+    d, keep = batch.desc()
+    bs = np.ascontiguousarray(batch.bs, dtype=np.float64)
+    kmin = np.ascontiguousarray(batch.kmin, dtype=np.float64)
     rho2 = np.zeros(batch.nsys * N * nt)
     reach0 = np.zeros((batch.nsys, 3), dtype=np.int32)
-    memo = {}
-    for s in range(batch.nsys):
-        fw = int(batch.framework_of[s]) - 1
-        Bs = float(batch.bs[fw])
-        cs = float(batch.constant_offset[fw])
-        natoms = int(batch.atom_offsets[fw + 1] - batch.atom_offsets[fw])
-        nk = int(batch.k_offsets[fw + 1] - batch.k_offsets[fw])
-        n = N * natoms + nk + 8
-        safety = 2 * n * eps_F * (Bs + abs(cs)) + 4.0e-6 * Bs
-        margin = math.inf if math.isinf(Bs) else (theta + 2) * kT + safety + Bs - cs
-        if not margin > 0:
-            raise ArgumentError(f"build_rejection_tables: system {s + 1} has margin={margin} <= 0 (Bs={Bs}, "
-                                f"safety={safety}, constant_offset={cs}, kT={kT}, theta_F={theta}); no valid "
-                                "rejection radius exists")
-        key = (fw, margin)
-        if key not in memo:
-            gt = batch.guest_types - 1
-            sg = batch.sigma[gt][:, :].reshape(-1)      # (N*nt) site-major
-            ep = batch.epsilon[gt][:, :].reshape(-1)
-            km = batch.kmin[fw * N * nt:(fw + 1) * N * nt]
-            memo[key] = find_rho2(sg, ep, km, margin, batch.cutoff)
-        r2 = memo[key]
-        rho2[s * N * nt:(s + 1) * N * nt] = r2
-        L = perpendicular_lengths(batch.cells[fw])
-        reach0[s] = stencil_reaches(L, batch.ncells[fw], math.sqrt(float(np.max(r2))) if len(r2) else 0.0)
+    bad = _lib.ctypes.c_int32(0)
+    st = _lib.lib().pa_rejection_tables(_lib.ctypes.byref(d), _lib.ptr(bs), _lib.ptr(kmin), float(kT),
+                                        float(np.finfo(batch.T).eps), _lib.ptr(rho2), _lib.ptr(reach0),
+                                        _lib.ctypes.byref(bad))
+    if st != _lib.PA_OK:
+        s = bad.value
+        raise ArgumentError(f"build_rejection_tables: system {s} has no valid rejection radius (margin <= 0 or a "
+                            f"root search failed; kT={kT}, theta_F={float(theta_F(np.float64))})")
     return rho2, reach0
 
 
