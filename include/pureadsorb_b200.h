@@ -56,8 +56,9 @@ const char* pa_last_error(const pa_context* ctx);
 /* Enables per-kernel CUDA-event timing inside pa_widom (adds events, no synchronisation). */
 pa_status pa_context_set_timing(pa_context* ctx, int32_t enable);
 /* Total device milliseconds and launch counts per kernel class since timing was enabled.
- * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy, 3 reduction, 4 neighbour-list build. */
-pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*5*/, int64_t* launches /*5*/);
+ * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy, 3 reduction, 4 neighbour-list build,
+ * 5 adjoint (selection, recomputation, reciprocal charge term). */
+pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*6*/, int64_t* launches /*6*/);
 
 /*
  * The fields of a `FrameworkBatch` (src/batch.jl:72-104), as raw arrays. natoms = Σ atoms
@@ -186,6 +187,33 @@ pa_status pa_rejection_tables(const pa_batch_desc* desc, const double* bs, const
  * come before any stream capture. */
 pa_status pa_widom_static(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
                           pa_insertion_out* per_insertion);
+
+/* Adjoint sums of one widom call; no counterpart in the reference, which has no gradients.
+ * The Julia analogue is a ChainRulesCore rrule of ln K_H over the FrameworkBatch fields sigma,
+ * epsilon and charges. With x_i = -ΔU_i/kT, m_s = max x over system s's survivors of this call
+ * and w_i = exp(x_i - m_s), d ln K_H(s) / dθ = -(Σ_i w_i ∂ΔU_i/∂θ) / (kT Σ_i w_i). The library
+ * returns the numerator sums for θ = the batch's pair tables and stored charges; the caller
+ * adds the constant offset's dependence (tail correction, net-charge term) and folds the
+ * pair tables onto per-type parameters (Lorentz-Berthelot). The sums are taken over every
+ * survivor whose x_i >= m_s - window (0 selects 50, i.e. relative weights down to 2e-22);
+ * lighter insertions are left out. Accumulation is FP32 per lane and FP64 across lanes and
+ * insertions by atomic adds, so the last bits depend on scheduling. */
+typedef struct pa_grad_sums {
+    double* xmax;        /* nsys out: m_s (-inf for a system without survivors)               */
+    double* sum_w;       /* nsys out: Σ_i w_i over every survivor of the call                  */
+    double* d_epsilon;   /* nsys*N*nt out: [s][a][t] Σ_i w_i ∂ΔU_i/∂ε(guest type of site a, t) */
+    double* d_sigma;     /* nsys*N*nt out: the same for σ                                      */
+    double* d_charge;    /* Σ_s natoms(framework_of[s]) out: Σ_i w_i ∂ΔU_i/∂q_j per stored
+                            atom j of the system's framework (desc order), system-major          */
+    double* s_guest;     /* optional, 2*Σ_s nk(framework_of[s]): Σ_i w_i S_g,i(k) (re, im)      */
+    double window;       /* in: selection window in units of kT (0: 50)                         */
+    int64_t recomputed;  /* out: insertions the adjoint pass recomputed                         */
+} pa_grad_sums;
+
+/* pa_widom plus the adjoint sums. FP32 batches only (the adjoint walks the FP32 path's bins and
+ * neighbour lists). Arguments as for pa_widom; sums->segments and per_insertion may be given. */
+pa_status pa_widom_grad(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
+                        pa_grad_sums* grad, pa_insertion_out* per_insertion);
 
 /* Host-side pose of insertion k of system s (the same stream as the device), for callers that
  * need the poses without a GPU (e.g. the self-term orientations of FrameworkBatch). precision

@@ -1023,3 +1023,140 @@ int32_t or_rejection_tables(const or_batch_view* b, const double* bs, const doub
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Adjoint sums. PureAdsorb.jl has no gradients; this is the derivative of its insertion_energy
+// (src/energy.jl:42-82) with respect to the pair tables and the stored charges, weighted by the
+// Boltzmann factors of one widom call (the reweighting identity
+// d ln <W> / dθ = -<W ∂ΔU/∂θ> / (kT <W>)), in FP64 over every survivor.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+void grad_insertion(const or_batch_view& b, int fw, const double* pos, const double* q, double w, double* d_eps,
+                    double* d_sig, double* d_q, double* sg) {
+    const int N = b.nguest, nt = b.ntypes;
+    double gs[3 * 16];
+    for (int s = 0; s < N; ++s) rotate_strict<double>(q, b.guest_sites + 3 * s, gs + 3 * s);
+    const double* A = b.cells + 9 * fw; const double* invA = b.invcells + 9 * fw;
+    const double rl2 = b.cutoff * b.cutoff, re2 = b.ewald_cutoff * b.ewald_cutoff, alpha = b.alphas[fw];
+    const int32_t a0 = b.atom_offsets[fw];
+    for (int32_t j = a0; j < b.atom_offsets[fw + 1]; ++j) {
+        double D0[3] = {pos[0] - b.positions[3 * j], pos[1] - b.positions[3 * j + 1], pos[2] - b.positions[3 * j + 2]};
+        minimum_image_strict<double>(A, invA, D0);
+        const int ht = b.types[j] - 1;
+        for (int s = 0; s < N; ++s) {
+            double D[3] = {D0[0] + gs[3 * s], D0[1] + gs[3 * s + 1], D0[2] + gs[3 * s + 2]};
+            double r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+            const int gt = b.guest_types[s] - 1;
+            if (r2 < rl2) {
+                const double sig = b.sigma[gt + nt * ht], eps = b.epsilon[gt + nt * ht];
+                double x = sig * sig / r2; x = x * x * x;
+                d_eps[s * nt + ht] += w * 4 * x * (x - 1);
+                if (sig > 0) d_sig[s * nt + ht] += w * 24 * eps / sig * x * (2 * x - 1);
+            }
+            if (r2 < re2) {
+                const double r = std::sqrt(r2);
+                d_q[j - a0] += w * KE * b.guest_charges[s] * std::erfc(alpha * r) / r;
+            }
+        }
+    }
+    const int32_t k0 = b.k_offsets[fw];
+    for (int32_t i = k0; i < b.k_offsets[fw + 1]; ++i) {
+        const double* k = b.ks + 3 * i;
+        double re = 0, im = 0;
+        for (int s = 0; s < N; ++s) {
+            double ph = k[0] * (pos[0] + gs[3 * s]) + k[1] * (pos[1] + gs[3 * s + 1]) + k[2] * (pos[2] + gs[3 * s + 2]);
+            re += b.guest_charges[s] * std::cos(ph); im += b.guest_charges[s] * std::sin(ph);
+        }
+        sg[2 * (i - k0)] += w * re;
+        sg[2 * (i - k0) + 1] += w * im;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Adjoint sums of one or_widom call, from its per-insertion outputs (system-major order; poses
+// as fractional position + quaternion). Per system s: xmax = max over survivors of x = -ΔU/kT,
+// sum_w = Σ w, w = exp(x - xmax); d_eps/d_sig [s][a][t] = Σ w ∂ΔU/∂(pair table entry of site a's
+// type and host type t); d_charge (system-major, natoms of the system's framework) = Σ w ∂ΔU/∂q_j,
+// real-space and reciprocal parts; s_guest (optional, 2 per k-vector) = Σ w S_g(k).
+int or_grad_sums(const or_batch_view* bp, double kT, int64_t ninsert, int64_t run, const double* poses,
+                 const double* dU, const uint8_t* flags, double* xmax, double* sum_w, double* d_eps, double* d_sig,
+                 double* d_charge, double* s_guest, int32_t nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    const or_batch_view& b = *bp;
+    const int N = b.nguest, nt = b.ntypes, nsys = b.nsys;
+    if (N > 16) return 1;
+    std::vector<int64_t> ns = system_counts(ninsert, nsys, run);
+    std::vector<int64_t> off(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) off[s + 1] = off[s] + ns[s];
+    int64_t aoff = 0, koff = 0;
+    for (int s = 0; s < nsys; ++s) {
+        const int fw = b.framework_of[s] - 1;
+        const int32_t na = b.atom_offsets[fw + 1] - b.atom_offsets[fw], nk = b.k_offsets[fw + 1] - b.k_offsets[fw];
+        double m = -INFINITY;
+        for (int64_t i = off[s]; i < off[s + 1]; ++i)
+            if (!flags[i]) m = std::max(m, -dU[i] / kT);
+        xmax[s] = m;
+        const size_t per = size_t(2 * N * nt + na + 2 * nk);
+        int nth = 1;
+#ifdef _OPENMP
+        nth = omp_get_max_threads();
+#endif
+        std::vector<double> buf(per * nth, 0.0), wsum(nth, 0.0);
+#pragma omp parallel
+        {
+            int th = 0;
+#ifdef _OPENMP
+            th = omp_get_thread_num();
+#endif
+            double* my = buf.data() + per * th;
+#pragma omp for schedule(static)
+            for (int64_t i = off[s]; i < off[s + 1]; ++i) {
+                if (flags[i] || m == -INFINITY) continue;
+                const double w = std::exp(-dU[i] / kT - m);
+                if (w == 0) continue;
+                wsum[th] += w;
+                const double* p = poses + 7 * i;
+                double pos[3];
+                matvec(b.cells + 9 * fw, p, pos);
+                grad_insertion(b, fw, pos, p + 3, w, my, my + N * nt, my + 2 * N * nt, my + 2 * N * nt + na);
+            }
+        }
+        double W = 0;
+        std::vector<double> tot(per, 0.0);
+        for (int t = 0; t < nth; ++t) {
+            W += wsum[t];
+            for (size_t x = 0; x < per; ++x) tot[x] += buf[per * t + x];
+        }
+        sum_w[s] = W;
+        for (int x = 0; x < N * nt; ++x) {
+            d_eps[int64_t(s) * N * nt + x] = tot[x];
+            d_sig[int64_t(s) * N * nt + x] = tot[N * nt + x];
+        }
+        const double* G = tot.data() + 2 * N * nt + na;
+        const int32_t a0 = b.atom_offsets[fw], k0 = b.k_offsets[fw];
+#pragma omp parallel for schedule(static)
+        for (int32_t j = 0; j < na; ++j) {
+            const double* r = b.positions + 3 * (a0 + j);
+            double acc = 0;
+            for (int32_t i = 0; i < nk; ++i) {
+                const double* k = b.ks + 3 * (k0 + i);
+                const double ph = k[0] * r[0] + k[1] * r[1] + k[2] * r[2];
+                acc += 2 * b.kprefactor[k0 + i] * (std::cos(ph) * G[2 * i] + std::sin(ph) * G[2 * i + 1]);
+            }
+            d_charge[aoff + j] = tot[2 * N * nt + j] + KE * acc;
+        }
+        if (s_guest)
+            for (int32_t i = 0; i < 2 * nk; ++i) s_guest[2 * koff + i] = G[i];
+        aoff += na;
+        koff += nk;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -69,6 +69,8 @@ def lib():
                                                      _p, _p, _p, _f64, _i64, _p, _p, _p]),
             "or_hardcore_flags": (None, [ctypes.POINTER(BatchView), _i32, _i32, _i64, _p, _p, _p, _p, _i32, _p]),
             "or_rejection_tables": (_i32, [ctypes.POINTER(BatchView), _p, _p, _f64, _f64, _p, _p]),
+            "or_grad_sums": (ctypes.c_int, [ctypes.POINTER(BatchView), _f64, _i64, _i64, _p, _p, _p, _p, _p, _p, _p,
+                                            _p, _p, _i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -262,6 +264,28 @@ def widom(v, precision, kT, ninsert, seed, nblocks, run, reject, rho2=None, reac
     if want_insertions:
         out.update(dU=dU, flags=flags, poses=poses_out)
     return out
+
+
+def grad_sums(v, kT, ninsert, run, out, natoms_of, nk_of, nthreads=0):
+    """Adjoint sums of one widom() result (its dU, flags and poses, system-major): per system
+    xmax, sum_w, d_eps/d_sig (N x nt), d_charge (the system's framework atoms) and s_guest
+    (complex per k-vector). natoms_of/nk_of: per-system atom and k-vector counts."""
+    nsys, N, nt = v.nsys, v.nguest, v.ntypes
+    na, nk = int(np.sum(natoms_of)), int(np.sum(nk_of))
+    xmax, sum_w = np.zeros(nsys), np.zeros(nsys)
+    d_eps, d_sig = np.zeros(nsys * N * nt), np.zeros(nsys * N * nt)
+    d_q, sg = np.zeros(na), np.zeros(2 * nk)
+    dU, flags, poses = c64(out["dU"]), np.ascontiguousarray(out["flags"], dtype=np.uint8), c64(out["poses"])
+    st = lib().or_grad_sums(ctypes.byref(v), kT, ninsert, run, P(poses), P(dU), P(flags), P(xmax), P(sum_w),
+                            P(d_eps), P(d_sig), P(d_q), P(sg), nthreads)
+    if st != 0:
+        raise ValueError(f"or_grad_sums failed ({st})")
+    aoff = np.concatenate([[0], np.cumsum(natoms_of)]).astype(np.int64)
+    koff = np.concatenate([[0], np.cumsum(nk_of)]).astype(np.int64)
+    sgc = sg[0::2] + 1j * sg[1::2]
+    return [dict(xmax=xmax[s], sum_w=sum_w[s], d_epsilon=d_eps.reshape(nsys, N, nt)[s],
+                 d_sigma=d_sig.reshape(nsys, N, nt)[s], d_charge=d_q[aoff[s]:aoff[s + 1]],
+                 s_guest=sgc[koff[s]:koff[s + 1]]) for s in range(nsys)]
 
 
 def insertion_energy(v, fw, pos, quat):

@@ -12,8 +12,10 @@ from .ewald import EwaldParams, ewald_alpha, ewald_kmax, full_ktables, kvectors,
 from .forcefield import ForceField, Guest, read_forcefield, read_guest, tail_delta
 from .structure import Framework, cartesian, natoms, read_cif, replicate, total_charge
 from . import synthetic
+from . import adjoint
+from .adjoint import WidomGrad, fold_replicas, widom_grad
 from .widom import (B200Backend, WidomResult, _reduce, _widom, block_sums, boltzmann_weight, build_rejection_tables,
                     default_run, sys_of_index, system_counts, widom, widom_singlephase)
 
 __all__ = ["Framework", "read_cif", "replicate", "ForceField", "read_forcefield", "Guest", "read_guest",
-           "EwaldParams", "FrameworkBatch", "widom", "WidomResult", "B200Backend"]
+           "EwaldParams", "FrameworkBatch", "widom", "WidomResult", "B200Backend", "widom_grad", "WidomGrad"]

@@ -55,6 +55,11 @@ class InsertionOut(ctypes.Structure):
     _fields_ = [("dU", _p), ("flags", _p), ("poses", _p)]
 
 
+class GradSums(ctypes.Structure):
+    _fields_ = [("xmax", _p), ("sum_w", _p), ("d_epsilon", _p), ("d_sigma", _p), ("d_charge", _p),
+                ("s_guest", _p), ("window", _f64), ("recomputed", _i64)]
+
+
 # (name, restype, argtypes): every entry point the header declares
 SIGNATURES = [
     ("pa_context_create", _i32, [_i32, ctypes.POINTER(_p)]),
@@ -68,6 +73,8 @@ SIGNATURES = [
     ("pa_batch_info", _i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     ("pa_widom", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
     ("pa_widom_static", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
+    ("pa_widom_grad", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(GradSums),
+                             ctypes.POINTER(InsertionOut)]),
     ("pa_rejection_tables", _i32, [ctypes.POINTER(BatchDesc), _p, _p, _f64, _f64, _p, _p, ctypes.POINTER(_i32)]),
     ("pa_segment_count", _i32, [_i64, _i32, _i32, _i32, ctypes.POINTER(_i64)]),
     ("pa_combine_segments", _i32, [_i64, _i32, _i32, _i32, _p, ctypes.POINTER(BlockSums)]),
@@ -163,8 +170,8 @@ class Context:
         self.check(lib().pa_context_set_timing(self.handle, int(bool(enable))), "pa_context_set_timing")
 
     def kernel_times(self):
-        ms = np.zeros(5)
-        n = np.zeros(5, dtype=np.int64)
+        ms = np.zeros(6)
+        n = np.zeros(6, dtype=np.int64)
         self.check(lib().pa_context_kernel_times(self.handle, ptr(ms), ptr(n)), "pa_context_kernel_times")
         return ms, n
 

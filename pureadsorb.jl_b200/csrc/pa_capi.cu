@@ -21,7 +21,7 @@ static_assert(PA_SEGMENT_SIZE == PA_SEGMENT, "segment size mismatch");
 
 namespace {
 
-constexpr int NCLASS = 5;  // kernel classes for timing: pose, scan/scatter, energy, reduce, lists
+constexpr int NCLASS = 6;  // kernel classes for timing: pose, scan/scatter, energy, reduce, lists, adjoint
 constexpr double LIST_PAD = 32;
 constexpr double DEFAULT_BIN_WIDTH = 3.0;  // Angstrom, FP32 path spatial bins
 constexpr double WAIT_LIMIT_S = 600.0;      // host-side bound on one call's device work
@@ -56,6 +56,8 @@ struct pa_context {
     // per-call workspace (grow-only)
     DevMem pose_a, pose_b, bin_of, slot, sorted, dU, bin_count, fine_start, bin_start, tile_start, counters, seg_out, seg_rng,
         sys_off, rho2, reach0;
+    // adjoint workspace
+    DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
 };
 
 struct pa_batch {
@@ -70,6 +72,11 @@ struct pa_batch {
     void* lists = nullptr;
     pa::DevBatch<float> d32{};
     pa::DevBatch<double> d64{};
+    // for the adjoint: FP64 fractional coordinates of the stored atoms (FP32 batches), 2 kpref per
+    // k-vector (inside the arena), and the (site, type) pair parameters of the desc
+    const double* frac64 = nullptr;
+    const double* kpref2 = nullptr;
+    std::vector<double> site_sigma, site_eps;
     // cudaFree returns stream-ordered pool memory synchronously, so the next upload reuses it
     ~pa_batch() {
         if (arena) cudaFree(arena);
@@ -210,8 +217,8 @@ pa_status wait_stream(pa_context* ctx) {
 
 struct Slots {
     size_t framework_of, cells, invcells, alphas, const_offset, atom_offsets, atoms, types, ncells, cell_offsets,
-        cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, sig2, eps4, bin_dims, bin_base, bin_fw;
-    size_t list_offsets, list_xyzq, list_type;  // offsets inside the list allocation
+        cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, kpref2, sig2, eps4, bin_dims, bin_base, bin_fw;
+    size_t list_offsets, list_xyzq, list_type, list_atom;  // offsets inside the list allocation
 };
 
 template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc, const Slots& o) {
@@ -251,6 +258,7 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     d.list_offsets = l ? reinterpret_cast<const int32_t*>(l + o.list_offsets) : nullptr;
     d.list_xyzq = l ? reinterpret_cast<const float4*>(l + o.list_xyzq) : nullptr;
     d.list_type = l ? reinterpret_cast<const int32_t*>(l + o.list_type) : nullptr;
+    d.list_atom = l ? reinterpret_cast<const int32_t*>(l + o.list_atom) : nullptr;
 }
 
 template <typename F>
@@ -274,12 +282,13 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     const int64_t ncoff = desc->cellgrid_offsets[nfw];
     std::vector<int32_t> coff(desc->cell_offsets, desc->cell_offsets + ncoff);
     std::vector<int32_t> cgo(desc->cellgrid_offsets, desc->cellgrid_offsets + nfw + 1);
-    std::vector<double> kvec(desc->ks, desc->ks + 3 * nk), kS2(2 * nk);
+    std::vector<double> kvec(desc->ks, desc->ks + 3 * nk), kS2(2 * nk), kpref2(nk);
     std::vector<float4> kcoef4(nk);
     std::vector<float> kstep(nfw, 1.0f);
     for (int64_t i = 0; i < nk; ++i) {
         kS2[2 * i] = 2 * desc->kprefactor[i] * desc->Shost[2 * i];
         kS2[2 * i + 1] = 2 * desc->kprefactor[i] * desc->Shost[2 * i + 1];
+        kpref2[i] = 2 * desc->kprefactor[i];
     }
     for (int fw = 0; fw < nfw; ++fw) {
         const int32_t k0 = B->k_offsets[fw], k1 = B->k_offsets[fw + 1];
@@ -308,12 +317,16 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         }
     }
     std::vector<F> sig2(N * nt), eps4(N * nt);
+    B->site_sigma.assign(N * nt, 0.0);
+    B->site_eps.assign(N * nt, 0.0);
     for (int a = 0; a < N; ++a) {
         int gt = desc->guest_types[a] - 1;
         for (int t = 0; t < nt; ++t) {
             double s = desc->sigma[gt + nt * t], e = desc->epsilon[gt + nt * t];
             sig2[a * nt + t] = F(s * s);
             eps4[a * nt + t] = F(4 * e);
+            B->site_sigma[a * nt + t] = s;
+            B->site_eps[a * nt + t] = e;
         }
     }
     // spatial bins
@@ -360,7 +373,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.const_offset = pk.add(co); o.atom_offsets = pk.add(B->atom_offsets); o.atoms = pk.add(atoms);
     o.types = pk.add(types); o.ncells = pk.add(ncells); o.cell_offsets = pk.add(coff);
     o.cellgrid_offsets = pk.add(cgo); o.k_offsets = pk.add(B->k_offsets); o.kvec = pk.add(kvec);
-    o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.sig2 = pk.add(sig2);
+    o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.kpref2 = pk.add(kpref2); o.sig2 = pk.add(sig2);
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
     const bool lists = sizeof(F) == 4;
     size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0;
@@ -389,6 +402,8 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.host.size(), st));
     PA_CUDA(ctx, cudaMemcpyAsync(B->arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
     char* base = static_cast<char*>(B->arena);
+    B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
+    if (lists) B->frac64 = reinterpret_cast<const double*>(base + t_frac);
     if (lists) {
         // neighbour lists: count pass, padded offsets on the host, fill pass
         pa::ListGeom g{};
@@ -425,12 +440,14 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         o.list_offsets = 0;
         o.list_xyzq = up256(sizeof(int32_t) * loff.size());
         o.list_type = up256(o.list_xyzq + sizeof(float4) * nent);
-        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_type + sizeof(int32_t) * nent, st));
+        o.list_atom = up256(o.list_type + sizeof(int32_t) * nent);
+        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_atom + sizeof(int32_t) * nent, st));
         PA_CUDA(ctx, cudaMemcpyAsync(B->lists, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st));
         char* lb = static_cast<char*>(B->lists);
         g.offsets = reinterpret_cast<const int32_t*>(lb + o.list_offsets);
         g.xyzq = reinterpret_cast<float4*>(lb + o.list_xyzq);
         g.type_out = reinterpret_cast<int32_t*>(lb + o.list_type);
+        g.atom_out = reinterpret_cast<int32_t*>(lb + o.list_atom);
         if (B->nbins > 0) {
             Timer tm(ctx, 4);
             pa::k_lists<true><<<B->nbins, 256, 0, st>>>(g);
@@ -469,6 +486,19 @@ cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::W
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
+    return cudaGetLastError();
+}
+
+template <int NS>
+cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, const pa::GradArgs& g,
+                        int32_t num_sms, cudaStream_t st) {
+    const size_t dyn = sizeof(float) * size_t(NS) * size_t(B->ntypes) * (1 + 2 * PA_WARPSG);
+    if (dyn > 227 * 1024) return cudaErrorInvalidValue;
+    if (dyn > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(pa::k_grad32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+        if (e != cudaSuccess) return e;
+    }
+    pa::k_grad32<NS><<<num_sms * 8, 32 * PA_WARPSG, dyn, st>>>(B->d32, ca, w, g);
     return cudaGetLastError();
 }
 
@@ -753,6 +783,121 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         const Seg& g = segs[sb + q];
         combine_segment(sums, g.s * nblocks + g.b, g.i1 - g.i0, seg_out.data() + 3 * q);
     }
+    return PA_OK;
+}
+
+pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args* args, pa_block_sums* sums,
+                        pa_grad_sums* grad, pa_insertion_out* per) {
+    if (!ctx || !B || !args || !sums || !grad) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->precision != PA_PRECISION_F32) return fail(ctx, PA_ERR_ARG, "pa_widom_grad needs a batch uploaded for PA_PRECISION_F32");
+    if (!grad->xmax || !grad->sum_w || !grad->d_epsilon || !grad->d_sigma || !grad->d_charge)
+        return fail(ctx, PA_ERR_ARG, "null adjoint output array");
+    if (!(grad->window >= 0)) return fail(ctx, PA_ERR_ARG, "window must be >= 0");
+    pa_status stt = pa_widom(ctx, B, args, sums, per);
+    if (stt != PA_OK) return stt;
+    const int nsys = B->nsys, N = B->nguest, nt = B->ntypes;
+    const int64_t nblocks = args->nblocks;
+    // call range (as in pa_widom)
+    std::vector<int64_t> ns = system_counts(args->ninsert, nsys, args->run);
+    std::vector<int64_t> off(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) off[s + 1] = off[s] + ns[s];
+    std::vector<Seg> segs = segments(ns, off, nblocks);
+    const int64_t nseg_all = int64_t(segs.size());
+    const int64_t sb = std::max<int64_t>(0, args->segment_begin);
+    const int64_t se = args->segment_end <= 0 ? nseg_all : std::min(args->segment_end, nseg_all);
+    // per-system shift and total weight from the block sums
+    std::vector<double> xmax(nsys, -INFINITY), sw(nsys, 0.0);
+    for (int s = 0; s < nsys; ++s)
+        for (int64_t b = 0; b < nblocks; ++b) xmax[s] = std::max(xmax[s], sums->lse_max[s * nblocks + b]);
+    for (int s = 0; s < nsys; ++s)
+        for (int64_t b = 0; b < nblocks; ++b) {
+            const double m = sums->lse_max[s * nblocks + b];
+            if (m != -INFINITY) sw[s] += sums->sum_w[s * nblocks + b] * std::exp(m - xmax[s]);
+        }
+    std::vector<int64_t> aoff(nsys + 1, 0), koff(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+        const int fw = B->framework_of[s] - 1;  // 1-based in the desc
+        aoff[s + 1] = aoff[s] + (B->atom_offsets[fw + 1] - B->atom_offsets[fw]);
+        koff[s + 1] = koff[s] + (B->k_offsets[fw + 1] - B->k_offsets[fw]);
+    }
+    const int64_t nlj = int64_t(nsys) * 2 * N * nt;
+    for (int s = 0; s < nsys; ++s) { grad->xmax[s] = xmax[s]; grad->sum_w[s] = sw[s]; }
+    std::fill(grad->d_epsilon, grad->d_epsilon + int64_t(nsys) * N * nt, 0.0);
+    std::fill(grad->d_sigma, grad->d_sigma + int64_t(nsys) * N * nt, 0.0);
+    std::fill(grad->d_charge, grad->d_charge + aoff[nsys], 0.0);
+    if (grad->s_guest) std::fill(grad->s_guest, grad->s_guest + 2 * koff[nsys], 0.0);
+    grad->recomputed = 0;
+    if (sb >= se) return PA_OK;
+    const int64_t i_lo = segs[sb].i0, n_act = segs[se - 1].i1 - i_lo;
+    const double window = grad->window > 0 ? grad->window : 50.0;
+    cudaStream_t st = ctx->stream;
+    PA_CUDA(ctx, ctx->heavy.ensure(sizeof(int32_t) * n_act));
+    PA_CUDA(ctx, ctx->g_w.ensure(sizeof(double) * nsys));
+    PA_CUDA(ctx, ctx->g_lj.ensure(sizeof(double) * nlj));
+    PA_CUDA(ctx, ctx->g_q.ensure(sizeof(double) * std::max<int64_t>(1, aoff[nsys])));
+    PA_CUDA(ctx, ctx->g_k.ensure(sizeof(double) * 2 * std::max<int64_t>(1, koff[nsys])));
+    PA_CUDA(ctx, upload(ctx->xmax, xmax, st));
+    PA_CUDA(ctx, upload(ctx->sys_aoff, aoff, st));
+    PA_CUDA(ctx, upload(ctx->sys_koff, koff, st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->g_w.p, 0, sizeof(double) * nsys, st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->g_lj.p, 0, sizeof(double) * nlj, st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->g_q.p, 0, sizeof(double) * std::max<int64_t>(1, aoff[nsys]), st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->g_k.p, 0, sizeof(double) * 2 * std::max<int64_t>(1, koff[nsys]), st));
+    PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.as<int32_t>() + 4, 0, sizeof(int32_t), st));
+    pa::Work w{};
+    w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>();
+    w.bin_of = ctx->bin_of.as<int32_t>(); w.dU = ctx->dU.as<double>();
+    pa::CallArgs ca{};
+    ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
+    ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
+    pa::GradArgs g{};
+    g.xmax = ctx->xmax.as<double>(); g.kT = args->kT; g.window = window;
+    g.sys_aoff = ctx->sys_aoff.as<int64_t>(); g.sys_koff = ctx->sys_koff.as<int64_t>(); g.nsys = nsys;
+    g.heavy = ctx->heavy.as<int32_t>(); g.nheavy = ctx->counters.as<int32_t>() + 4;
+    g.g_w = ctx->g_w.as<double>(); g.g_lj = ctx->g_lj.as<double>(); g.g_q = ctx->g_q.as<double>();
+    g.g_k = ctx->g_k.as<double>(); g.frac = B->frac64; g.kpref2 = B->kpref2;
+    {
+        Timer tm(ctx, 5);
+        pa::k_heavy<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, ca, g);
+        PA_CUDA(ctx, cudaGetLastError());
+        cudaError_t e = cudaSuccess;
+        PA_DISPATCH_NS(N, (e = launch_grad<NSV>(B, ca, w, g, ctx->num_sms, st)));
+        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("adjoint kernel launch: ") + cudaGetErrorString(e));
+        int nl = 2;
+        if (B->nk > 0) {
+            int32_t amax = 0;
+            for (int fw = 0; fw < B->nfw; ++fw) amax = std::max(amax, B->atom_offsets[fw + 1] - B->atom_offsets[fw]);
+            if (amax > 0 && nsys <= 65535) {
+                pa::k_charge_recip<<<dim3(unsigned((amax + 255) / 256), unsigned(nsys)), 256, 0, st>>>(B->d32, g);
+                PA_CUDA(ctx, cudaGetLastError());
+                ++nl;
+            } else if (amax > 0) {
+                return fail(ctx, PA_ERR_ARG, "pa_widom_grad supports at most 65535 systems");
+            }
+        }
+        tm.stop(nl);
+    }
+    std::vector<double> glj(nlj);
+    int32_t nh = 0;
+    PA_CUDA(ctx, cudaMemcpyAsync(glj.data(), ctx->g_lj.p, sizeof(double) * nlj, cudaMemcpyDeviceToHost, st));
+    if (aoff[nsys] > 0)
+        PA_CUDA(ctx, cudaMemcpyAsync(grad->d_charge, ctx->g_q.p, sizeof(double) * aoff[nsys], cudaMemcpyDeviceToHost, st));
+    if (grad->s_guest && koff[nsys] > 0)
+        PA_CUDA(ctx, cudaMemcpyAsync(grad->s_guest, ctx->g_k.p, sizeof(double) * 2 * koff[nsys], cudaMemcpyDeviceToHost, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(&nh, ctx->counters.as<int32_t>() + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    if (ctx->timing) Timer::collect(ctx);
+    grad->recomputed = nh;
+    // ∂u/∂ε = 4 x(x - 1), ∂u/∂σ = (24 ε/σ) x(2x - 1) for the (site, type) pair parameters
+    for (int s = 0; s < nsys; ++s)
+        for (int a = 0; a < N; ++a)
+            for (int t = 0; t < nt; ++t) {
+                const int64_t o = (int64_t(s) * N + a) * nt + t;
+                const double sg = B->site_sigma[a * nt + t], ep = B->site_eps[a * nt + t];
+                grad->d_epsilon[o] = 4.0 * glj[(int64_t(s) * 2 * N + a) * nt + t];
+                grad->d_sigma[o] = sg > 0 ? 24.0 * ep / sg * glj[(int64_t(s) * 2 * N + N + a) * nt + t] : 0.0;
+            }
     return PA_OK;
 }
 

@@ -61,6 +61,7 @@ struct DevBatch {
     const int32_t* list_offsets;                  // nbins+1, multiples of PA_LIST_PAD
     const float4* list_xyzq;                      // imaged position relative to the bin centre, charge
     const int32_t* list_type;                     // 0-based type (padding entries: type 0, far away)
+    const int32_t* list_atom;                     // stored-atom index of each entry
 };
 
 // Per-call arguments shared by the kernels.
@@ -346,6 +347,7 @@ __device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
 }
 
 #include "pa_energy32.cuh"
+#include "pa_grad32.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // k_energy64: the plain FP64 form of the reference algorithm (src/energy.jl:42-82): for every
@@ -527,6 +529,7 @@ struct ListGeom {
     const int32_t* offsets;    // nbins+1 (fill pass)
     float4* xyzq;
     int32_t* type_out;
+    int32_t* atom_out;         // stored-atom index of each entry (for the adjoint)
 };
 
 template <bool FILL>
@@ -579,6 +582,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
             if (pos < g.offsets[bin + 1]) {
                 g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
                 g.type_out[pos] = g.types[j];
+                g.atom_out[pos] = j;
             }
         }
         __syncthreads();
@@ -591,6 +595,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         for (int32_t q = s_base + threadIdx.x; q < end; q += blockDim.x) {
             g.xyzq[q] = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.0f);
             g.type_out[q] = 0;
+            g.atom_out[q] = 0;
         }
     }
 }

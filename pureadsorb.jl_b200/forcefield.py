@@ -102,3 +102,43 @@ def tail_delta(ff, counts, guest_counts, V):
             c = tail_coefficient(ff, a, b)
             acc += 2 * counts[a] * guest_counts[b] * c + guest_counts[a] * guest_counts[b] * c
     return 8 * math.pi / 3 / V * acc
+
+
+def type_parameters(ff):
+    """Per-type (sigma, epsilon) of a Lorentz-Berthelot force field: the diagonals of its tables
+    (src/forcefield.jl:22-39 builds sigma_ii = sigma_i, epsilon_ii = epsilon_i)."""
+    return np.diag(ff.sigma).copy(), np.diag(ff.epsilon).copy()
+
+
+def pair_to_type_grad(ff, d_sigma_pair, d_epsilon_pair):
+    """Chain rule through Lorentz-Berthelot mixing: derivatives with respect to the pair tables
+    (d/dsigma_ij, d/depsilon_ij, full ntypes x ntypes matrices indexed like ff.sigma) to
+    derivatives with respect to the per-type parameters. sigma_ij = (sigma_i + sigma_j)/2 gives
+    d/dsigma_t = sum_ij d/dsigma_ij (delta_it + delta_jt)/2; epsilon_ij = sqrt(epsilon_i epsilon_j)
+    gives d/depsilon_t = sum_ij d/depsilon_ij epsilon_ij (delta_it + delta_jt)/(2 epsilon_t)
+    (unbounded at epsilon_t = 0 when another factor is nonzero)."""
+    dS = np.asarray(d_sigma_pair, dtype=np.float64)
+    dE = np.asarray(d_epsilon_pair, dtype=np.float64)
+    _, eps_t = type_parameters(ff)
+    g_sig = 0.5 * (dS.sum(axis=1) + dS.sum(axis=0))
+    wE = dE * ff.epsilon
+    with np.errstate(divide="ignore", invalid="ignore"):
+        g_eps = (wE.sum(axis=1) + wE.sum(axis=0)) / (2 * eps_t)
+    return g_sig, g_eps
+
+
+def tail_delta_pair_grad(ff, counts, guest_counts, V):
+    """Derivatives of tail_delta with respect to the pair tables (d/dsigma_ij, d/depsilon_ij) for
+    c_ij = epsilon_ij (s^12/(3 rc^9) - s^6/rc^3), s = sigma_ij, weighted like tail_delta by
+    2 counts_i guest_counts_j + guest_counts_i guest_counts_j (src/forcefield.jl:103-124)."""
+    n = ff.sigma.shape[0]
+    if not ff.tail:
+        return np.zeros((n, n)), np.zeros((n, n))
+    counts = np.asarray(counts, dtype=np.float64)
+    gc = np.asarray(guest_counts, dtype=np.float64)
+    M = 2 * counts[:, None] * gc[None, :] + gc[:, None] * gc[None, :]
+    s, e, rc = ff.sigma, ff.epsilon, ff.cutoff
+    f = 8 * math.pi / 3 / V
+    dE = f * M * (s**12 / (3 * rc**9) - s**6 / rc**3)
+    dS = f * M * e * (4 * s**11 / rc**9 - 6 * s**5 / rc**3)
+    return dS, dE

@@ -172,11 +172,12 @@ def _validate(batch, guest, ninsert, chunk, nblocks, run):
 
 
 def _widom(batch, guest, *, reject, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None,
-           insertions=None, segment_range=None, segments_out=None):
+           insertions=None, segment_range=None, segments_out=None, grad_sums=None):
     """The widom call with optional extras: `insertions` (a dict) receives per-insertion dU,
     flags and poses in system-major sample order; `segment_range` (begin, end) restricts the call
     to a contiguous range of PA_SEGMENT-insertion segments (a shard of a multi-GPU job), whose
-    segment triplets go into `segments_out` (an array of 3 per job segment)."""
+    segment triplets go into `segments_out` (an array of 3 per job segment); `grad_sums` (a
+    _lib.GradSums over caller-owned arrays) makes the call pa_widom_grad, which also fills it."""
     ninsert = int(ninsert)
     runlen, ns = _validate(batch, guest, ninsert, chunk, nblocks, run)
     T = float(T.magnitude) if hasattr(T, "magnitude") else float(T)
@@ -205,7 +206,10 @@ def _widom(batch, guest, *, reject, T, ninsert, backend=None, seed=0, chunk=2**1
         insertions["poses"] = np.zeros((ninsert, 7))
         out = _lib.InsertionOut(_lib.ptr(insertions["dU"]), _lib.ptr(insertions["flags"]),
                                 _lib.ptr(insertions["poses"]))
-    ctx.check(_lib.lib().pa_widom(ctx.handle, dev.handle, args, sums, out), "pa_widom")
+    if grad_sums is not None:
+        ctx.check(_lib.lib().pa_widom_grad(ctx.handle, dev.handle, args, sums, grad_sums, out), "pa_widom_grad")
+    else:
+        ctx.check(_lib.lib().pa_widom(ctx.handle, dev.handle, args, sums, out), "pa_widom")
     if segment_range is not None:
         return lse, sw, suw, cnt
     return _results(batch, kT, nblocks, lse, sw, suw, cnt)
