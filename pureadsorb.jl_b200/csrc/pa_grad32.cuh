@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
     const int32_t nwarps = gridDim.x * PA_WARPSG;
     for (int32_t h = blockIdx.x * PA_WARPSG + wp; h < nh; h += nwarps) {
         const int32_t li = g.heavy[h];
-        const int32_t bin = w.bin_of[li];
+        const int32_t bin = w.bin_of[li] / b.nsub;  // bin_of holds the sub-bin bin * nsub + octant
         const int32_t sy = find_system(ca.sys_off, g.nsys, ca.i_lo + li);
         const double wgt = exp(-w.dU[li] / g.kT - g.xmax[sy]);
         const int32_t fw = b.bin_fw[bin];

@@ -79,7 +79,7 @@ struct Work {
     float4* pose_b;    // quaternion
     double4* pose64a;  // FP64 path rpos (xyz)
     double4* pose64b;  // FP64 path quaternion
-    int32_t* bin_of;   // n_act: bin of a survivor, -1 if rejected
+    int32_t* bin_of;   // n_act: sub-bin of a survivor (bin * nsub + octant), -1 if rejected
     int32_t* slot;     // n_act
     int32_t* sorted;   // n_act: local insertion index in bin order
     double* dU;        // n_act: ΔU (+inf if rejected)
