@@ -40,6 +40,7 @@ def parse():
     p.add_argument("--ninsert", type=int, default=1_000_000)
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -295,6 +296,36 @@ def main():
                 e2e_ms.append(dt * 1e3)
         e2e_value = args.ninsert / (float(np.mean(e2e_ms)) / 1e3)
 
+        # the adjoint workload: widom plus d ln K_H / dθ (14 LJ parameters, 5,832 charges) over
+        # 4,000,000 insertions of the same framework
+        adj = None
+        if not args.no_adjoint and world == 1:
+            nadj = 4_000_000
+            ff = pa.synthetic.co2(T=np.float32)[1]
+            for _ in range(2):
+                pa.widom_grad(batch, guest, ff, T=prm["T"], ninsert=nadj, seed=prm["seed"], nblocks=nblocks,
+                              backend=backend)
+            torch.cuda.synchronize()
+            ctx.set_timing(True)
+            k0, n0 = ctx.kernel_times()
+            ms_adj = []
+            for _ in range(3):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                _, gr = pa.widom_grad(batch, guest, ff, T=prm["T"], ninsert=nadj, seed=prm["seed"], nblocks=nblocks,
+                                      backend=backend)
+                b.record(stream)
+                torch.cuda.synchronize()
+                ms_adj.append(a.elapsed_time(b))
+            k1, n1 = ctx.kernel_times()
+            ctx.set_timing(False)
+            ms_call = float(np.median(ms_adj))
+            adj = {"ninsert": nadj, "ms_per_call": ms_call, "value": nadj / (ms_call / 1e3), "unit": "insertions/s",
+                   "adjoint_kernel_ms_per_call": float((k1[5] - k0[5]) / 3), "recomputed": int(gr[0].recomputed),
+                   "parameters": int(2 * len(ff.names) + len(gr[0].charges)),
+                   "note": "widom_grad: forward pass + adjoint pass + host chain rule, CUDA events around the call"}
+
         cpu = None
         if not args.no_cpu:
             b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
@@ -318,6 +349,7 @@ def main():
                               "energy": kms[2] / args.steps, "segment_reduce": kms[3] / args.steps},
                 "roofline": roof,
                 "fp64_plain": fp64,
+                "adjoint": adj,
                 "e2e": {"value": e2e_value, "unit": "insertions/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
                 "cpu_baseline": cpu}
