@@ -184,10 +184,14 @@ def main():
         return pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=ninsert, seed=prm["seed"], nblocks=nblocks,
                          backend=backend, segment_range=(s0, s1), segments_out=segs)
 
+    # layout and launch shape chosen by the autotuner on this rank's own call, then every step
+    # replayed from a CUDA graph
+    tune = pa.autotune(batch, guest, T=prm["T"], ninsert=args.ninsert, backend=backend, seed=prm["seed"],
+                       nblocks=nblocks)
+    ctx.set_tuning(use_graphs=True)
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    ctx.set_timing(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
         torch.distributed.barrier()
@@ -203,6 +207,13 @@ def main():
         torch.distributed.barrier()
     ms_steps = [a.elapsed_time(b) for a, b in ev]
     ms_total = float(sum(ms_steps))
+    # per-kernel device times from a second pass of the same steps with kernel timing on (direct
+    # launches: graphs are not used while timing)
+    ctx.set_timing(True)
+    for i in range(args.steps):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
     kms, kn = ctx.kernel_times()
     ctx.set_timing(False)
     if world > 1:
@@ -344,6 +355,8 @@ def main():
                 "result": {"mu_ex": res32.mu_ex, "mu_ex_err": res32.mu_ex_err, "K_H": res32.K_H,
                            "K_H_err": res32.K_H_err, "q_st": res32.q_st, "q_st_err": res32.q_st_err},
                 "clocks": clk.summary(),
+                "tuning": {"bin_width": tune.bin_width, "ctas_per_sm": tune.ctas_per_sm, "cuda_graphs": True,
+                           "candidates": [list(r) for r in tune.table]},
                 "gpu_launches": int(5 * args.steps),
                 "kernel_ms": {"pose_phase0": kms[0] / args.steps, "scan_scatter": kms[1] / args.steps,
                               "energy": kms[2] / args.steps, "segment_reduce": kms[3] / args.steps},

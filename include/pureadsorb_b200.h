@@ -60,6 +60,21 @@ pa_status pa_context_set_timing(pa_context* ctx, int32_t enable);
  * 5 adjoint (selection, recomputation, reciprocal charge term). */
 pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*6*/, int64_t* launches /*6*/);
 
+/* Layout and launch choices of a context (no counterpart in the reference), set by the
+ * autotuner or by hand. bin_width: edge in Å of the FP32 path's spatial bins, applied to batches
+ * uploaded afterwards (0 selects 3.0). ctas_per_sm: persistent CTAs per SM of the FP32 energy
+ * kernel, 1..8 (0 selects 8). use_graphs: 1 makes pa_widom capture its device sequence (kernels,
+ * memsets and the copy of the segment sums into pinned host memory) in a CUDA graph and replay it
+ * while the call's shape (batch, insertion range, workspace) repeats; seed and kT may change
+ * between replays. Graphs are not used while per-kernel timing is on. */
+typedef struct pa_tuning {
+    double bin_width;
+    int32_t ctas_per_sm;
+    int32_t use_graphs;
+} pa_tuning;
+pa_status pa_context_set_tuning(pa_context* ctx, const pa_tuning* tuning);
+pa_status pa_context_get_tuning(const pa_context* ctx, pa_tuning* tuning);
+
 /*
  * The fields of a `FrameworkBatch` (src/batch.jl:72-104), as raw arrays. natoms = Σ atoms
  * (atom_offsets[nfw]); nk = Σ k-vectors (k_offsets[nfw]); N = nguest; nt = ntypes.

@@ -14,6 +14,7 @@ from .structure import Framework, cartesian, natoms, read_cif, replicate, total_
 from . import synthetic
 from . import adjoint
 from .adjoint import WidomGrad, fold_replicas, widom_grad
+from .tune import TuneReport, autotune
 from .widom import (B200Backend, WidomResult, _reduce, _widom, block_sums, boltzmann_weight, build_rejection_tables,
                     default_run, sys_of_index, system_counts, widom, widom_singlephase)
 

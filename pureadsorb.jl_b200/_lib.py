@@ -55,6 +55,10 @@ class InsertionOut(ctypes.Structure):
     _fields_ = [("dU", _p), ("flags", _p), ("poses", _p)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("bin_width", _f64), ("ctas_per_sm", _i32), ("use_graphs", _i32)]
+
+
 class GradSums(ctypes.Structure):
     _fields_ = [("xmax", _p), ("sum_w", _p), ("d_epsilon", _p), ("d_sigma", _p), ("d_charge", _p),
                 ("s_guest", _p), ("window", _f64), ("recomputed", _i64)]
@@ -68,6 +72,8 @@ SIGNATURES = [
     ("pa_last_error", ctypes.c_char_p, [_p]),
     ("pa_context_set_timing", _i32, [_p, _i32]),
     ("pa_context_kernel_times", _i32, [_p, _p, _p]),
+    ("pa_context_set_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
+    ("pa_context_get_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
     ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
     ("pa_batch_free", _i32, [_p]),
     ("pa_batch_info", _i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
@@ -168,6 +174,23 @@ class Context:
 
     def set_timing(self, enable):
         self.check(lib().pa_context_set_timing(self.handle, int(bool(enable))), "pa_context_set_timing")
+
+    def set_tuning(self, bin_width=None, ctas_per_sm=None, use_graphs=None):
+        """Changes the given launch choices (pa_tuning); the others keep their values. A new
+        bin width applies to batches uploaded afterwards."""
+        t = self.tuning()
+        if bin_width is not None:
+            t.bin_width = float(bin_width)
+        if ctas_per_sm is not None:
+            t.ctas_per_sm = int(ctas_per_sm)
+        if use_graphs is not None:
+            t.use_graphs = int(bool(use_graphs))
+        self.check(lib().pa_context_set_tuning(self.handle, ctypes.byref(t)), "pa_context_set_tuning")
+
+    def tuning(self):
+        t = Tuning()
+        self.check(lib().pa_context_get_tuning(self.handle, ctypes.byref(t)), "pa_context_get_tuning")
+        return t
 
     def kernel_times(self):
         ms = np.zeros(6)

@@ -58,6 +58,25 @@ struct pa_context {
         sys_off, rho2, reach0;
     // adjoint workspace
     DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
+    // launch choices, the replayable graph of the last call's device sequence and its key
+    pa_tuning tuning{0.0, 0, 0};
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
+    // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
+    // counters, and host copies of the last uploaded per-call tables (re-uploaded only on change)
+    DevMem scal;
+    double* h_seg = nullptr;
+    size_t h_seg_cap = 0;
+    int32_t* h_cnt = nullptr;
+    std::vector<int64_t> up_seg_rng, up_sys_off;
+    std::vector<int32_t> up_reach0;
+    std::vector<unsigned char> up_rho2;
+    std::vector<double> up_scal;
+    ~pa_context() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (h_seg) cudaFreeHost(h_seg);
+        if (h_cnt) cudaFreeHost(h_cnt);
+    }
 };
 
 struct pa_batch {
@@ -103,6 +122,19 @@ cudaError_t upload(DevMem& m, const std::vector<T>& v, cudaStream_t st) {
     cudaError_t e = m.ensure(v.size() * sizeof(T));
     if (e != cudaSuccess || v.empty()) return e;
     return cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// Uploads v unless the device copy already holds exactly the same contents (cache = the host
+// copy of the last upload into m).
+template <typename T>
+cudaError_t upload_cached(DevMem& m, std::vector<T>& cache, const std::vector<T>& v, cudaStream_t st) {
+    if (m.p && cache.size() == v.size() && m.bytes >= v.size() * sizeof(T) &&
+        (v.empty() || std::memcmp(cache.data(), v.data(), v.size() * sizeof(T)) == 0))
+        return cudaSuccess;
+    cache.clear();
+    cudaError_t e = upload(m, v, st);
+    if (e == cudaSuccess) cache = v;
+    return e;
 }
 
 // Host staging of many small device tables into one buffer (256-byte aligned slots), uploaded
@@ -339,8 +371,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
                                     desc->guest_sites[3 * a + 1] * desc->guest_sites[3 * a + 1] +
                                     desc->guest_sites[3 * a + 2] * desc->guest_sites[3 * a + 2]));
     const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
-    double binw = DEFAULT_BIN_WIDTH;
-    if (const char* s = std::getenv("PA_BIN_WIDTH")) { double v = std::atof(s); if (v > 0.5) binw = v; }
+    double binw = ctx->tuning.bin_width > 0 ? ctx->tuning.bin_width : DEFAULT_BIN_WIDTH;
     for (int fw = 0; fw < nfw; ++fw) {
         double L[3];
         perpendicular_lengths(desc->cells + 9 * fw, L);
@@ -469,20 +500,28 @@ void launch_pose(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, c
     pa::k_pose<F, NS><<<grid, 256, 0, st>>>(d, ca, w, rho2, reach0);
 }
 
+// Raises the energy kernel's dynamic shared-memory limit when the batch's type tables need it
+// (a function attribute, set before any stream capture).
 template <int NS>
-cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms, cudaStream_t st) {
+cudaError_t prepare_energy(const pa_batch* B) {
+    if (B->precision != PA_PRECISION_F32) return cudaSuccess;
+    const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
+    if (dyn <= 48 * 1024) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    return e;
+}
+
+template <int NS>
+cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms, int32_t ctas,
+                          cudaStream_t st) {
     if (B->precision == PA_PRECISION_F32) {
-        size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
-        if (dyn > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(pa::k_energy32<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-            if (e != cudaSuccess) return e;
-        }
+        const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
+        const int32_t per = (ctas >= 1 && ctas <= PA_CTAS_PER_SM32) ? ctas : PA_CTAS_PER_SM32;
         if (B->d32.rl2 == B->d32.re2)
-            pa::k_energy32<NS, true><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+            pa::k_energy32<NS, true><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
         else
-            pa::k_energy32<NS, false><<<num_sms * PA_CTAS_PER_SM32, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+            pa::k_energy32<NS, false><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
@@ -564,6 +603,21 @@ pa_status pa_context_set_timing(pa_context* ctx, int32_t enable) {
     if (!ctx) return PA_ERR_ARG;
     ctx->timing = enable != 0;
     for (int c = 0; c < NCLASS; ++c) { ctx->ms[c] = 0; ctx->launches[c] = 0; }
+    return PA_OK;
+}
+
+pa_status pa_context_set_tuning(pa_context* ctx, const pa_tuning* t) {
+    if (!ctx || !t) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (!(t->bin_width == 0 || (t->bin_width >= 1.0 && t->bin_width <= 50.0)))
+        return fail(ctx, PA_ERR_ARG, "bin_width must be 0 or within [1, 50] Angstrom");
+    if (t->ctas_per_sm < 0 || t->ctas_per_sm > PA_CTAS_PER_SM32) return fail(ctx, PA_ERR_ARG, "ctas_per_sm must be within [0, 8]");
+    ctx->tuning = *t;
+    return PA_OK;
+}
+
+pa_status pa_context_get_tuning(const pa_context* ctx, pa_tuning* t) {
+    if (!ctx || !t) return PA_ERR_ARG;
+    *t = ctx->tuning;
     return PA_OK;
 }
 
@@ -692,17 +746,33 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     PA_CUDA(ctx, ctx->tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
     PA_CUDA(ctx, ctx->counters.ensure(sizeof(int32_t) * 8));
     PA_CUDA(ctx, ctx->seg_out.ensure(sizeof(double) * 3 * nseg));
-    PA_CUDA(ctx, upload(ctx->seg_rng, seg_rng, st));
-    PA_CUDA(ctx, upload(ctx->sys_off, off, st));
+    // per-call tables, uploaded only when they differ from the last call's
+    PA_CUDA(ctx, upload_cached(ctx->seg_rng, ctx->up_seg_rng, seg_rng, st));
+    PA_CUDA(ctx, upload_cached(ctx->sys_off, ctx->up_sys_off, off, st));
     if (args->reject) {
         std::vector<int32_t> r0(args->reach0, args->reach0 + 3 * nsys);
-        PA_CUDA(ctx, upload(ctx->reach0, r0, st));
+        PA_CUDA(ctx, upload_cached(ctx->reach0, ctx->up_reach0, r0, st));
         const int64_t nr = int64_t(nsys) * N * nt;
-        if (f32) { std::vector<float> r2(nr); for (int64_t q = 0; q < nr; ++q) r2[q] = float(args->rho2[q]); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
-        else { std::vector<double> r2(args->rho2, args->rho2 + nr); PA_CUDA(ctx, upload(ctx->rho2, r2, st)); }
+        std::vector<unsigned char> r2(nr * (f32 ? sizeof(float) : sizeof(double)));
+        if (f32) { float* p = reinterpret_cast<float*>(r2.data()); for (int64_t q = 0; q < nr; ++q) p[q] = float(args->rho2[q]); }
+        else std::memcpy(r2.data(), args->rho2, nr * sizeof(double));
+        PA_CUDA(ctx, upload_cached(ctx->rho2, ctx->up_rho2, r2, st));
     }
-    PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
-    PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 8, st));
+    {
+        const uint64_t seed = args->seed;
+        std::vector<double> sv(2);
+        std::memcpy(&sv[0], &seed, sizeof(double));
+        sv[1] = args->kT;
+        PA_CUDA(ctx, upload_cached(ctx->scal, ctx->up_scal, sv, st));
+    }
+    // pinned staging for the segment sums and counters (a graph copies into it)
+    if (ctx->h_seg_cap < size_t(3 * nseg)) {
+        if (ctx->h_seg) cudaFreeHost(ctx->h_seg);
+        ctx->h_seg = nullptr; ctx->h_seg_cap = 0;
+        PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_seg), sizeof(double) * 3 * nseg));
+        ctx->h_seg_cap = size_t(3 * nseg);
+    }
+    if (!ctx->h_cnt) PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_cnt), sizeof(int32_t) * 8));
     pa::Work w{};
     if (f32) { w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>(); }
     else { w.pose64a = ctx->pose_a.as<double4>(); w.pose64b = ctx->pose_b.as<double4>(); }
@@ -713,37 +783,91 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     pa::CallArgs ca{};
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
+    ca.seed_dev = ctx->scal.as<uint64_t>(); ca.kT_dev = ctx->scal.as<double>() + 1;
     {
-        Timer tm(ctx, 0);
-        if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, ctx->rho2.as<float>(), ctx->reach0.as<int32_t>(), st))); }
-        else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, ctx->rho2.as<double>(), ctx->reach0.as<int32_t>(), st))); }
-        tm.stop(1);
-        PA_CUDA(ctx, cudaGetLastError());
-    }
-    {
-        Timer tm(ctx, 1);
-        pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
-        pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
-        tm.stop(2);
-        PA_CUDA(ctx, cudaGetLastError());
-    }
-    {
-        Timer tm(ctx, 2);
         cudaError_t e = cudaSuccess;
-        PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, st)));
-        tm.stop(1);
-        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+        PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
+        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel attributes: ") + cudaGetErrorString(e));
     }
-    {
-        Timer tm(ctx, 3);
-        pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT);
-        tm.stop(1);
-        PA_CUDA(ctx, cudaGetLastError());
+    const int32_t ctas = ctx->tuning.ctas_per_sm;
+    // the device sequence of one call: memsets, pose + phase 0, scan, scatter, energy, segment
+    // sums, and the copies of the segment sums and counters into pinned host memory
+    auto enqueue = [&]() -> pa_status {
+        PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
+        PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 8, st));
+        {
+            Timer tm(ctx, 0);
+            if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, ctx->rho2.as<float>(), ctx->reach0.as<int32_t>(), st))); }
+            else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, ctx->rho2.as<double>(), ctx->reach0.as<int32_t>(), st))); }
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
+        }
+        {
+            Timer tm(ctx, 1);
+            pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
+            pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
+            tm.stop(2);
+            PA_CUDA(ctx, cudaGetLastError());
+        }
+        {
+            Timer tm(ctx, 2);
+            cudaError_t e = cudaSuccess;
+            PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, ctas, st)));
+            tm.stop(1);
+            if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+        }
+        {
+            Timer tm(ctx, 3);
+            pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT, ca.kT_dev);
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
+        }
+        PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_seg, ctx->seg_out.p, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_cnt, ctx->counters.p, sizeof(int32_t) * 8, cudaMemcpyDeviceToHost, st));
+        return PA_OK;
+    };
+    if (ctx->tuning.use_graphs && !ctx->timing) {
+        // the key: everything a captured launch depends on besides seed and kT, i.e. the kernel
+        // arguments (the batch's device view byte for byte, so a re-upload of the same batch into
+        // the same pooled addresses replays) and the workspace addresses
+        struct GraphKey {
+            const void* ptrs[19];
+            int64_t i_lo, n_act, nseg, nfine;
+            int32_t nbins, N, f32, reject, ctas, pad;
+        } key;
+        std::memset(&key, 0, sizeof(key));
+        const void* ps[19] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
+                              ctx->bin_count.p, ctx->fine_start.p, ctx->bin_start.p, ctx->tile_start.p, ctx->counters.p,
+                              ctx->seg_out.p, ctx->seg_rng.p, ctx->sys_off.p, ctx->rho2.p, ctx->reach0.p, ctx->scal.p,
+                              ctx->h_seg};
+        std::memcpy(key.ptrs, ps, sizeof(ps));
+        key.i_lo = i_lo; key.n_act = n_act; key.nseg = nseg; key.nfine = nfine;
+        key.nbins = B->nbins; key.N = N; key.f32 = f32 ? 1 : 0; key.reject = ca.reject; key.ctas = ctas;
+        const unsigned char* kp = reinterpret_cast<const unsigned char*>(&key);
+        std::vector<unsigned char> kb(kp, kp + sizeof(key));
+        const unsigned char* vp = f32 ? reinterpret_cast<const unsigned char*>(&B->d32) : reinterpret_cast<const unsigned char*>(&B->d64);
+        kb.insert(kb.end(), vp, vp + (f32 ? sizeof(B->d32) : sizeof(B->d64)));
+        if (!ctx->gexec || kb != ctx->gkey) {
+            if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+            ctx->gkey.clear();
+            cudaGraph_t graph = nullptr;
+            PA_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            pa_status es = enqueue();
+            cudaError_t ee = cudaStreamEndCapture(st, &graph);
+            if (es != PA_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+            PA_CUDA(ctx, ee);
+            cudaError_t ie = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) { ctx->gexec = nullptr; PA_CUDA(ctx, ie); }
+            ctx->gkey = kb;
+        }
+        PA_CUDA(ctx, cudaGraphLaunch(ctx->gexec, st));
+    } else {
+        pa_status es = enqueue();
+        if (es != PA_OK) return es;
     }
-    std::vector<double> seg_out(3 * nseg);
-    int32_t counters[8];
-    PA_CUDA(ctx, cudaMemcpyAsync(seg_out.data(), ctx->seg_out.p, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
-    PA_CUDA(ctx, cudaMemcpyAsync(counters, ctx->counters.p, sizeof(counters), cudaMemcpyDeviceToHost, st));
+    const double* seg_out = ctx->h_seg;
+    const int32_t* counters = ctx->h_cnt;
     std::vector<int32_t> bin_of;
     std::vector<char> pose_a, pose_b;
     if (per && per->dU)
@@ -781,7 +905,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             for (int r = 0; r < 3; ++r) sums->segments[3 * (sb + q) + r] = seg_out[3 * q + r];
     for (int64_t q = 0; q < nseg; ++q) {
         const Seg& g = segs[sb + q];
-        combine_segment(sums, g.s * nblocks + g.b, g.i1 - g.i0, seg_out.data() + 3 * q);
+        combine_segment(sums, g.s * nblocks + g.b, g.i1 - g.i0, seg_out + 3 * q);
     }
     return PA_OK;
 }
@@ -1130,10 +1254,11 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     PA_CUDA(ctx, cudaGetLastError());
     {
         cudaError_t e = cudaSuccess;
-        PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, st)));
+        PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
+        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
     }
-    pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT);
+    pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT, nullptr);
     PA_CUDA(ctx, cudaGetLastError());
     PA_CUDA(ctx, cudaMemcpyAsync(st_segout, base + ST_SEG_OUT, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
     PA_CUDA(ctx, cudaMemcpyAsync(st_counters, base + ST_COUNTERS, sizeof(st_counters), cudaMemcpyDeviceToHost, st));

@@ -71,6 +71,10 @@ struct CallArgs {
     uint64_t seed;
     int32_t reject;
     double kT;
+    // optional device copies of seed and kT: when set the kernels read these instead, so a
+    // launch sequence captured in a CUDA graph replays for any seed and temperature
+    const uint64_t* seed_dev;
+    const double* kT_dev;
 };
 
 // Per-call device workspace.
@@ -193,7 +197,7 @@ __global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w
     const int64_t k = i - ca.sys_off[s] + 1;
     const int32_t fw = b.framework_of[s];
     F rp[3], qt[4];
-    draw_pose<F>(ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    draw_pose<F>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
     if (sizeof(F) == 4) {
         w.pose_a[t] = make_float4(float(rp[0]), float(rp[1]), float(rp[2]), 0.0f);
         w.pose_b[t] = make_float4(float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3]));
@@ -457,7 +461,8 @@ __global__ void __launch_bounds__(PA_TILE64) k_energy64(DevBatch<double> b, Call
 // weight is exactly zero contribute zero, as in boltzmann_weight). 256 threads, 8 consecutive
 // insertions per thread summed in order, then a fixed shuffle/shared-memory tree.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_segsum(Work w, double kT) {
+__global__ void __launch_bounds__(256) k_segsum(Work w, double kT, const double* kT_dev) {
+    if (kT_dev) kT = *kT_dev;
     __shared__ double s_red[3][8];
     const int64_t b0 = w.seg_rng[2 * blockIdx.x], b1 = w.seg_rng[2 * blockIdx.x + 1];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;

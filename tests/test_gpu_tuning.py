@@ -1,0 +1,78 @@
+"""Launch choices on the B200: CUDA-graph replay, bin width and CTAs per SM change how the work is
+laid out, never the results. Graph replays equal direct launches bit for bit (also when the seed
+changes between replays); other bin widths keep poses and phase-0 flags exact and energies within
+the FP32 tolerance of the parity tests; the autotuner leaves its choice set on the context."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import F32_ABS, F32_REL
+
+pytestmark = pytest.mark.gpu
+
+NINS = 40_000
+NBLOCKS = 4
+
+
+@pytest.fixture(scope="module")
+def co2_batch(pa):
+    fws, ff, guest, ewald, _ = pa.synthetic.co2()
+    return pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32), guest
+
+
+def _call(pa, batch, guest, backend, seed):
+    ins = {}
+    raw = pa._widom(batch, guest, reject=True, T=298.15, ninsert=NINS, seed=seed, nblocks=NBLOCKS, backend=backend,
+                    insertions=ins, segment_range=(0, 0))
+    return raw, ins
+
+
+def test_graph_replay_equals_direct_launch(pa, co2_batch):
+    batch, guest = co2_batch
+    be = pa.B200Backend(0)
+    direct = {s: _call(pa, batch, guest, be, s) for s in (5, 6)}
+    be.ctx.set_tuning(use_graphs=True)
+    for s in (5, 5, 6, 5):  # capture, replay, replay with another seed, and back
+        raw, ins = _call(pa, batch, guest, be, s)
+        for a, b in zip(raw, direct[s][0]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(ins["dU"], direct[s][1]["dU"])
+        assert np.array_equal(ins["flags"], direct[s][1]["flags"])
+    batch.drop_device()
+
+
+@pytest.mark.parametrize("width,ctas", [(2.5, 4), (5.0, 6)])
+def test_bin_width_and_grid_keep_results(pa, co2_batch, width, ctas):
+    batch, guest = co2_batch
+    be = pa.B200Backend(0)
+    _, ref = _call(pa, batch, guest, be, 11)
+    batch.drop_device()
+    be.ctx.set_tuning(bin_width=width, ctas_per_sm=ctas)
+    _, ins = _call(pa, batch, guest, be, 11)
+    batch.drop_device()
+    assert np.array_equal(ins["poses"], ref["poses"])
+    assert np.array_equal(ins["flags"], ref["flags"])
+    surv = ref["flags"] == 0
+    a, b = ins["dU"][surv], ref["dU"][surv]
+    assert np.all(np.abs(a - b) <= 2 * (F32_ABS + F32_REL * np.abs(b)))
+
+
+def test_autotune_sets_its_choice(pa, co2_batch):
+    batch, guest = co2_batch
+    be = pa.B200Backend(0)
+    before = pa.widom(batch, guest, T=298.15, ninsert=NINS, seed=3, nblocks=NBLOCKS, backend=be)
+    rep = pa.autotune(batch, guest, T=298.15, ninsert=NINS, backend=be, seed=3, nblocks=NBLOCKS,
+                      bin_widths=(3.0, 4.0), ctas_per_sm=(4, 8))
+    assert len(rep.table) == 4 and rep.ms == min(r[2] for r in rep.table)
+    t = be.ctx.tuning()
+    assert (t.bin_width, t.ctas_per_sm) == (rep.bin_width, rep.ctas_per_sm)
+    after = pa.widom(batch, guest, T=298.15, ninsert=NINS, seed=3, nblocks=NBLOCKS, backend=be)
+    assert np.log(after[0].K_H) == pytest.approx(np.log(before[0].K_H), abs=1e-4)
+    batch.drop_device()
+
+
+def test_tuning_rejects_bad_values(pa):
+    be = pa.B200Backend(0)
+    with pytest.raises(Exception, match="bin_width"):
+        be.ctx.set_tuning(bin_width=0.1)
+    with pytest.raises(Exception, match="ctas_per_sm"):
+        be.ctx.set_tuning(ctas_per_sm=9)
