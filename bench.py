@@ -41,6 +41,8 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-fit", action="store_true")
     return p.parse_args()
 
 
@@ -111,6 +113,31 @@ def workload(pa, T):
     return pa.FrameworkBatch(fws, ff, guest, ewald), guest, prm
 
 
+def count_pairs(batch, poses):
+    """Mean numbers of (site, atom) pairs inside the LJ and the Ewald cutoff per insertion, for
+    survivors' poses (fractional position, quaternion) of a one-framework batch: one minimum
+    image per atom, as the reference's insertion_energy visits them (numpy, FP64)."""
+    A = np.asarray(batch.cells[0])
+    iA = np.linalg.inv(A)
+    atoms = np.asarray(batch.positions)
+    sites = np.asarray(batch.guest_sites_orig)
+    rl2, re2 = batch.cutoff ** 2, batch.ewald_cutoff ** 2
+    nl = ne = 0
+    for p in poses:
+        pos = A @ p[:3]
+        u, w = p[3:6], p[6]
+        for g in sites:
+            t = 2 * np.cross(u, g)
+            r = pos + g + w * t + np.cross(u, t)
+            d = r - atoms
+            d -= (A @ np.rint(iA @ d.T)).T
+            r2 = np.einsum("ij,ij->i", d, d)
+            nl += int(np.sum(r2 < rl2))
+            ne += int(np.sum(r2 < re2))
+    n = max(1, len(poses))
+    return nl / n, ne / n
+
+
 def cpu_baseline_port(pa, orc, batch, guest, ninsert_full, target_s=12.0, nthreads=0):
     """Times the oracle (FP64 C++ restatement of the reference CPU path, OpenMP over the host
     cores) on a bounded sample of the same workload; returns (insertions/s, sample size, cores)."""
@@ -126,6 +153,96 @@ def cpu_baseline_port(pa, orc, batch, guest, ninsert_full, target_s=12.0, nthrea
         if dt > 0.25 * target_s or n >= ninsert_full:
             return n / dt, n, (nthreads or os.cpu_count())
         n = int(min(ninsert_full, n * max(2.0, 0.5 * target_s / max(dt, 1e-3))))
+
+
+def batched_workload(pa, backend, torch, stream, flush):
+    """64 uneven frameworks, 2^20 insertions each, in one call (one persistent energy launch over
+    all frameworks' bins), batch tables built with device structure factors, autotuned, replayed
+    from a CUDA graph; FP32 against the plain FP64 form on 2^14 insertions per framework."""
+    ctx = backend.ctx
+    fws, ff, guest, ewald, prm = pa.synthetic.batched(T=np.float32)
+    t0 = time.perf_counter()
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, sk=ctx.structure_factor)
+    build_s = time.perf_counter() - t0
+    n, T, seed, nb = prm["ninsert"], prm["T"], prm["seed"], prm["nblocks"]
+    tune = pa.autotune(b, guest, T=T, ninsert=n, backend=backend, seed=seed, nblocks=nb, bin_widths=(3.0, 3.5, 4.0),
+                       ctas_per_sm=(8,), repeats=1)
+    ctx.set_tuning(use_graphs=True)
+    pa._widom(b, guest, reject=True, T=T, ninsert=n, seed=seed, nblocks=nb, backend=backend, segment_range=(0, 0))
+    ms = []
+    for _ in range(3):
+        flush.zero_()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pa._widom(b, guest, reject=True, T=T, ninsert=n, seed=seed, nblocks=nb, backend=backend, segment_range=(0, 0))
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(e))
+    ms_call = float(np.median(ms))
+    # accuracy against the plain FP64 form, per framework, from the raw block sums (the generator
+    # can draw frameworks so dense that every insertion overlaps: W = 0 there, which widom's
+    # reduction reports as an error, so those are counted instead)
+    n64 = len(fws) * 2**14
+
+    def raw(batch):
+        lse, sw, suw, cnt = pa._widom(batch, guest, reject=True, T=T, ninsert=n64, seed=seed, nblocks=nb,
+                                      backend=backend, segment_range=(0, 0))
+        sW, sUW = pa.block_sums(lse, sw, suw)
+        W = sW.reshape(len(fws), nb).sum(axis=1)
+        UW = sUW.reshape(len(fws), nb).sum(axis=1)
+        return W, UW
+
+    b64 = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float64, sk=ctx.structure_factor)
+    raw(b64)
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    W64, UW64 = raw(b64)
+    e.record(stream)
+    torch.cuda.synchronize()
+    rate64 = n64 / (a.elapsed_time(e) / 1e3)
+    W32, UW32 = raw(b)
+    ok = (W64 > 0) & (W32 > 0)
+    dln = np.abs(np.log(W32[ok]) - np.log(W64[ok]))
+    dq = np.abs(UW32[ok] / W32[ok] - UW64[ok] / W64[ok])
+    b.drop_device()
+    b64.drop_device()
+    return {"workload": "batched_64_frameworks", "frameworks": len(fws), "natoms": int(len(b.positions)),
+            "coupled_k": int(b.k_offsets[-1]), "ninsert": n, "ms_per_call": ms_call, "value": n / (ms_call / 1e3),
+            "unit": "insertions/s", "batch_build_s": build_s, "tuning": {"bin_width": tune.bin_width,
+                                                                         "ctas_per_sm": tune.ctas_per_sm,
+                                                                         "cuda_graphs": True},
+            "fp64_plain": {"value": rate64, "ninsert": n64, "ratio_fp32_over_fp64": n / (ms_call / 1e3) / rate64,
+                           "max_dlnKH": float(np.max(dln)), "max_dqst_eV": float(np.max(dq)),
+                           "frameworks_compared": int(ok.sum()),
+                           "frameworks_without_accessible_volume": int(np.sum((W64 == 0) & (W32 == 0)))}}
+
+
+def fitting_workload(pa, backend):
+    """Adam on the 8 palette scale factors of 128 frameworks, 2^18 insertions per framework per
+    step (batched FP32 widom + adjoint), targets from the plain FP64 form at the hidden factors."""
+    ctx = backend.ctx
+    fws, ff, guest, ewald, prm = pa.synthetic.fitting(T=np.float32)
+    n, T, seed = len(fws) * prm["ninsert_per_framework"], prm["T"], prm["seed"]
+    t0 = time.perf_counter()
+    ffh = pa.fit.scaled_forcefield(ff, prm["fitted_types"], prm["hidden"])
+    targets = pa.fit.target_lnkh(fws, ffh, guest, ewald, T=T, ninsert=n, seed=seed, backend=backend,
+                                 sk=ctx.structure_factor)
+    target_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor)
+    build_s = time.perf_counter() - t0
+    res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
+                               lr=prm["lr"], seed=seed, backend=backend)
+    return {"workload": "fitting_128_frameworks_palette4", "frameworks": len(fws), "natoms": int(len(b.positions)),
+            "ninsert_per_step": n, "steps": prm["steps"], "lr": prm["lr"],
+            "frameworks_fitted": int(np.sum(np.isfinite(targets))),
+            "ms_per_step_median": float(np.median(res.ms)), "wall_s": float(np.sum(res.ms) / 1e3),
+            "loss_first": res.loss[0], "loss_last": res.loss[-1],
+            "max_scale_error_initial": float(np.max(np.abs(1 - prm["hidden"]))),
+            "max_scale_error_final": float(np.max(np.abs(res.x - prm["hidden"]))),
+            "scales_final": res.x.tolist(), "scales_hidden": prm["hidden"].tolist(),
+            "targets_s": target_s, "batch_build_s": build_s}
 
 
 def main():
@@ -242,12 +359,8 @@ def main():
         sample_n = 20_000
         pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=sample_n, seed=prm["seed"], nblocks=nblocks,
                   backend=backend, insertions=ins)
-        v, keep = orc.view(batch, batch.guest_sites_orig, batch.guest_charges_orig, batch.cutoff, batch.ewald_cutoff)
-        rho2, reach0 = pa.build_rejection_tables(batch, kT32)
-        ref = orc.widom(v, 32, kT32, sample_n, prm["seed"], nblocks, pa.default_run(sample_n, 1), True, rho2, reach0)
-        surv_frac = float(np.mean(ref["flags"] == 0))
-        nsurv_s = max(1, int(np.sum(ref["flags"] == 0)))
-        n_lj, n_ew = ref["pairs"][0] / nsurv_s, ref["pairs"][1] / nsurv_s
+        surv_frac = float(np.mean(ins["flags"] == 0))
+        n_lj, n_ew = count_pairs(batch, ins["poses"][ins["flags"] == 0][:512])
         dev = batch.device(ctx)
         list_entries, nbins = dev.info()
         L = list_entries / nbins
@@ -337,6 +450,9 @@ def main():
                    "parameters": int(2 * len(ff.names) + len(gr[0].charges)),
                    "note": "widom_grad: forward pass + adjoint pass + host chain rule, CUDA events around the call"}
 
+        batched = None if args.no_batched or world > 1 else batched_workload(pa, backend, torch, stream, flush)
+        fitting = None if args.no_fit or world > 1 else fitting_workload(pa, backend)
+
         cpu = None
         if not args.no_cpu:
             b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
@@ -363,6 +479,8 @@ def main():
                 "roofline": roof,
                 "fp64_plain": fp64,
                 "adjoint": adj,
+                "batched": batched,
+                "fitting": fitting,
                 "e2e": {"value": e2e_value, "unit": "insertions/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
                 "cpu_baseline": cpu}

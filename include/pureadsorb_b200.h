@@ -115,6 +115,21 @@ typedef struct pa_batch_desc {
  * FP32 path). Replaces `adapt(backend, batch)` (src/widom.jl:368). */
 pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t precision, pa_batch** out);
 pa_status pa_batch_free(pa_batch* batch);
+/* Replaces an uploaded batch's LJ pair tables and per-framework constant offsets in place: the
+ * parts of a FrameworkBatch that change when only the force field's LJ parameters do (a fitting
+ * loop). No counterpart in the reference, which rebuilds the whole batch. sigma and epsilon are
+ * nt*nt column-major as in pa_batch_desc; constant_offset has nfw entries. Geometry, bins,
+ * neighbour lists and k tables stay. Waits for the copies. */
+pa_status pa_batch_set_pair_tables(pa_context* ctx, pa_batch* batch, const double* sigma, const double* epsilon,
+                                   const double* constant_offset);
+/* Hard-core bound B_s of every framework of an uploaded batch (`hardcore_bound`,
+ * src/reject.jl:95-124, which FrameworkBatch computes on the host, src/batch.jl:409-423),
+ * evaluated on the device in FP64 from the batch's current pair tables: one root search per
+ * attractive (site, atom) pair and a fixed-order sum per framework. For callers that change the
+ * pair tables with pa_batch_set_pair_tables and need the bounds for pa_rejection_tables again.
+ * Agrees with the host computation to rounding (a different erfc and summation order). bs gets
+ * nfw values; PA_ERR_ARG when a root search fails. */
+pa_status pa_batch_hardcore_bounds(pa_context* ctx, const pa_batch* batch, double* bs);
 /* Size of the FP32 path's neighbour lists (entries over all bins) and the bin count. */
 pa_status pa_batch_info(const pa_batch* batch, int64_t* list_entries, int64_t* nbins);
 

@@ -15,6 +15,7 @@ from . import synthetic
 from . import adjoint
 from .adjoint import WidomGrad, fold_replicas, widom_grad
 from .tune import TuneReport, autotune
+from . import fit
 from .widom import (B200Backend, WidomResult, _reduce, _widom, block_sums, boltzmann_weight, build_rejection_tables,
                     default_run, sys_of_index, system_counts, widom, widom_singlephase)
 

@@ -76,6 +76,8 @@ SIGNATURES = [
     ("pa_context_get_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
     ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
     ("pa_batch_free", _i32, [_p]),
+    ("pa_batch_set_pair_tables", _i32, [_p, _p, _p, _p, _p]),
+    ("pa_batch_hardcore_bounds", _i32, [_p, _p, _p]),
     ("pa_batch_info", _i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     ("pa_widom", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
     ("pa_widom_static", _i32, [_p, _p, ctypes.POINTER(WidomArgs), ctypes.POINTER(BlockSums), ctypes.POINTER(InsertionOut)]),
@@ -220,6 +222,20 @@ class DeviceBatch:
         self.precision = precision
         self._keep = keep
         ctx.batches.add(self)
+
+    def set_pair_tables(self, sigma, epsilon, constant_offset):
+        """Replaces the LJ pair tables (nt x nt) and constant offsets (nfw) in place."""
+        sg = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64).T.reshape(-1))
+        ep = np.ascontiguousarray(np.asarray(epsilon, dtype=np.float64).T.reshape(-1))
+        co = np.ascontiguousarray(constant_offset, dtype=np.float64)
+        self.ctx.check(lib().pa_batch_set_pair_tables(self.ctx.handle, self.handle, ptr(sg), ptr(ep), ptr(co)),
+                       "pa_batch_set_pair_tables")
+
+    def hardcore_bounds(self, nfw):
+        """Hard-core bound of every framework from the uploaded pair tables, on the device."""
+        bs = np.zeros(nfw)
+        self.ctx.check(lib().pa_batch_hardcore_bounds(self.ctx.handle, self.handle, ptr(bs)), "pa_batch_hardcore_bounds")
+        return bs
 
     def info(self):
         a, b = _i64(), _i64()

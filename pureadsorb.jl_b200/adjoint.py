@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from .constants import KB, KE
 from .forcefield import pair_to_type_grad, tail_delta_pair_grad
-from .widom import _results, _widom, default_backend
+from .widom import _results, _widom, default_backend, lnkh_from_sums
 
 
 @dataclass
@@ -63,10 +63,11 @@ def assemble(batch, ff, s, sums, kT):
     dE = np.zeros((nff, nff))
     d_eps = np.asarray(sums["d_epsilon"], dtype=np.float64).reshape(len(gt), -1)
     d_sig = np.asarray(sums["d_sigma"], dtype=np.float64).reshape(len(gt), -1)
-    for a in range(len(gt)):
-        i = c2o[gt[a]]
-        np.add.at(dE, (i, c2o), d_eps[a] / W)
-        np.add.at(dS, (i, c2o), d_sig[a] / W)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for a in range(len(gt)):
+            i = c2o[gt[a]]
+            np.add.at(dE, (i, c2o), d_eps[a] / W)
+            np.add.at(dS, (i, c2o), d_sig[a] / W)
     # the tail correction shifts every insertion's ΔU by the same amount
     counts = np.bincount(c2o[np.asarray(batch.types[a0:a1], dtype=np.int64) - 1], minlength=nff)
     gcounts = np.bincount(np.asarray(batch.guest_types_orig, dtype=np.int64) - 1, minlength=nff)
@@ -76,7 +77,8 @@ def assemble(batch, ff, s, sums, kT):
     # constant offset, KE * (-pi/(2 V alpha^2)) * ((Qh + Qg)^2 - Qh^2), whose derivative is
     # KE * (-pi Qg / (V alpha^2)) for every host atom
     Qg = float(np.sum(batch.guest_charges_orig))
-    dq = np.asarray(sums["d_charge"], dtype=np.float64) / W + KE * (-math.pi * Qg / (V * alpha**2))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        dq = np.asarray(sums["d_charge"], dtype=np.float64) / W + KE * (-math.pi * Qg / (V * alpha**2))
     g_q = np.empty(a1 - a0)
     g_q[np.asarray(batch.perm[a0:a1], dtype=np.int64)] = -beta * dq
     return WidomGrad(-beta * g_eps, -beta * g_sig, g_q, int(sums.get("recomputed", 0)), W, float(sums["xmax"]))
@@ -91,12 +93,14 @@ def fold_replicas(g, natoms_unit):
 
 
 def widom_grad(batch, guest, ff, *, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None,
-               window=0.0):
+               window=0.0, reduce=True):
     """widom plus d ln K_H / dθ for every system: returns (results, grads), grads[s] a WidomGrad.
     θ: the per-type LJ ε and σ of `ff` (which must be the force field the batch was built from)
     and the charges of each framework's atoms. The batch must be FP32 (the adjoint walks the FP32
     path's neighbour lists). Insertions whose weight is below exp(-window) times their system's
-    largest are left out of the sums (0 selects 50)."""
+    largest are left out of the sums (0 selects 50). With reduce=False the first element is
+    ln K_H per system from the raw sums instead of the WidomResults (-inf, and NaN gradients,
+    for a system without accessible volume, where the reduction throws)."""
     nsys = batch.nsys
     N = len(batch.guest_types)
     nt = len(batch.sigma)
@@ -109,7 +113,8 @@ def widom_grad(batch, guest, ff, *, T, ninsert, backend=None, seed=0, chunk=2**1
     kT = float(batch.T(KB * T))
     lse, sw, suw, cnt = _widom(batch, guest, reject=True, T=T, ninsert=ninsert, backend=backend, seed=seed,
                                chunk=chunk, nblocks=nblocks, run=run, segment_range=(0, 0), grad_sums=gs)
-    results = _results(batch, kT, nblocks, lse, sw, suw, cnt)
+    results = _results(batch, kT, nblocks, lse, sw, suw, cnt) if reduce else \
+        lnkh_from_sums(batch, kT, nblocks, lse, sw, suw, cnt)
     aoff = np.concatenate([[0], np.cumsum(nat)]).astype(np.int64)
     grads = []
     for s in range(nsys):

@@ -6,6 +6,7 @@ constants and accumulation, or the plain FP64 path - as the reference's float ty
 Index conventions follow the reference exactly: offsets are 0-based, LJ types, guest types and
 framework indices 1-based.
 """
+import copy
 import math
 
 import numpy as np
@@ -129,6 +130,7 @@ class FrameworkBatch:
         constant_offset, halfranges = [], []
         ncells, cell_offsets, cellgrid_offsets = [], [], [0]
         kmin = []
+        offset_parts = []  # per framework: (KE (self + excl + net), self-term mean, type counts, V)
         natoms_total = 0
         for n, fw in enumerate(unique, start=1):
             m = min_multiplicity(fw.cell, rc_guard)
@@ -197,6 +199,7 @@ class FrameworkBatch:
             Qg = float(np.sum(guest.charges))
             net = -math.pi / (2 * V * alpha**2) * ((Qh + Qg) ** 2 - Qh**2)
             constant_offset.append(tail_delta(ff, counts, gcounts, V) + KE * (self_e + excl + net) + self_mean)
+            offset_parts.append((KE * (self_e + excl + net), self_mean, counts, V))
 
         self.positions = np.ascontiguousarray(np.concatenate(positions) if natoms_total else np.zeros((0, 3)))
         self.types = np.ascontiguousarray(np.concatenate(types) if natoms_total else np.zeros(0, np.int32), dtype=np.int32)
@@ -230,15 +233,54 @@ class FrameworkBatch:
         self.nsys = len(fws)
         self.framework_of = np.array(framework_of, dtype=np.int32)
         self.perm = np.concatenate(perms) if perms else np.zeros(0, np.int32)
-        # hardcore bound per framework (src/batch.jl:409-423)
-        self.bs = np.empty(len(unique))
-        for n in range(len(unique)):
+        self._ff_names = list(ff.names)
+        self._gcounts = gcounts
+        self._offset_parts = offset_parts
+        self.bs = self._hardcore_bounds()
+        self._device = {}
+
+    def _hardcore_bounds(self):
+        """B_s per framework (src/batch.jl:409-423)."""
+        bs = np.empty(self.nframeworks())
+        for n in range(len(bs)):
             a0, a1 = self.atom_offsets[n], self.atom_offsets[n + 1]
             k0, k1 = self.k_offsets[n], self.k_offsets[n + 1]
-            self.bs[n] = hardcore_bound(self.guest_types, guest.charges, sigma, epsilon, self.types[a0:a1],
-                                        self.charges[a0:a1], ff.cutoff, alpha, self.kprefactor[k0:k1],
-                                        self.Shost[k0:k1])
-        self._device = {}
+            bs[n] = hardcore_bound(self.guest_types, self.guest_charges_orig, self.sigma, self.epsilon,
+                                   self.types[a0:a1], self.charges[a0:a1], self.cutoff, float(self.alphas[n]),
+                                   self.kprefactor[k0:k1], self.Shost[k0:k1])
+        return bs
+
+    def with_forcefield(self, ff, move_device=False, device_bounds=False):
+        """The same frameworks, guest and Ewald tables under another force field with the same type
+        names, cutoff and tail setting (a fitting loop changes only LJ parameters). Recomputes what
+        depends on them: the compact pair tables, each framework's constant offset (its tail
+        correction) and hard-core bound; the rest is shared with this batch. The result equals a
+        fresh FrameworkBatch(fws, ff, guest, ewald) field for field. With move_device=True the new
+        batch takes over this batch's device uploads, whose pair tables and constant offsets are
+        replaced in place (pa_batch_set_pair_tables), and this batch loses them. With
+        device_bounds=True as well, the hard-core bounds come from the device
+        (pa_batch_hardcore_bounds; equal to the host's to rounding) instead of the host loop."""
+        if list(ff.names) != self._ff_names:
+            raise ArgumentError("with_forcefield needs a force field with the same type names")
+        if float(ff.cutoff) != self.cutoff:
+            raise ArgumentError(f"with_forcefield needs the same LJ cutoff ({self.cutoff}), got {ff.cutoff}")
+        new = copy.copy(self)
+        ci = np.asarray(self.compact_to_orig, dtype=np.int64) - 1
+        new.sigma = ff.sigma[np.ix_(ci, ci)].copy()
+        new.epsilon = ff.epsilon[np.ix_(ci, ci)].copy()
+        new.constant_offset = np.array([tail_delta(ff, counts, self._gcounts, V) + ke + sm
+                                        for ke, sm, counts, V in self._offset_parts])
+        new._device = {}
+        if move_device:
+            for key, dev in self._device.items():
+                dev.set_pair_tables(new.sigma, new.epsilon, new.constant_offset)
+                new._device[key] = dev
+            self._device = {}
+        if device_bounds and new._device:
+            new.bs = next(iter(new._device.values())).hardcore_bounds(new.nframeworks())
+        else:
+            new.bs = new._hardcore_bounds()
+        return new
 
     def nframeworks(self):
         return len(self.cells)

@@ -64,7 +64,7 @@ struct pa_context {
     std::vector<unsigned char> gkey;
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
     // counters, and host copies of the last uploaded per-call tables (re-uploaded only on change)
-    DevMem scal;
+    DevMem scal, bnd;
     double* h_seg = nullptr;
     size_t h_seg_cap = 0;
     int32_t* h_cnt = nullptr;
@@ -96,6 +96,12 @@ struct pa_batch {
     const double* frac64 = nullptr;
     const double* kpref2 = nullptr;
     std::vector<double> site_sigma, site_eps;
+    std::vector<int32_t> guest_types;  // 0-based compact type of each guest site
+    std::vector<double> guest_q;       // guest site charges
+    std::vector<double> recip_bound;   // per framework Σ_k kpref |S_k| (hard-core bound)
+    double cutoff = 0;                 // LJ cutoff
+    const double* q64 = nullptr;       // FP64 charges of the stored atoms (inside the arena)
+    const int32_t* types0 = nullptr;   // 0-based types (inside the arena)
     // cudaFree returns stream-ordered pool memory synchronously, so the next upload reuses it
     ~pa_batch() {
         if (arena) cudaFree(arena);
@@ -405,6 +411,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.types = pk.add(types); o.ncells = pk.add(ncells); o.cell_offsets = pk.add(coff);
     o.cellgrid_offsets = pk.add(cgo); o.k_offsets = pk.add(B->k_offsets); o.kvec = pk.add(kvec);
     o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.kpref2 = pk.add(kpref2); o.sig2 = pk.add(sig2);
+    const size_t t_q64 = pk.add(std::vector<double>(desc->charges, desc->charges + na));
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
     const bool lists = sizeof(F) == 4;
     size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0;
@@ -434,6 +441,8 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     PA_CUDA(ctx, cudaMemcpyAsync(B->arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
     char* base = static_cast<char*>(B->arena);
     B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
+    B->q64 = reinterpret_cast<const double*>(base + t_q64);
+    B->types0 = reinterpret_cast<const int32_t*>(base + o.types);
     if (lists) B->frac64 = reinterpret_cast<const double*>(base + t_frac);
     if (lists) {
         // neighbour lists: count pass, padded offsets on the host, fill pass
@@ -553,6 +562,30 @@ cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Wor
         default: { constexpr int NSV = 8; EXPR; } break;     \
     }
 
+template <typename F>
+pa_status set_pair_tables_impl(pa_context* ctx, pa_batch* B, const double* sigma, const double* epsilon,
+                               const double* constant_offset) {
+    const int N = B->nguest, nt = B->ntypes;
+    std::vector<F> sig2(N * nt), eps4(N * nt);
+    for (int a = 0; a < N; ++a) {
+        const int gt = B->guest_types[a];
+        for (int t = 0; t < nt; ++t) {
+            const double sg = sigma[gt + nt * t], e = epsilon[gt + nt * t];
+            sig2[a * nt + t] = F(sg * sg);
+            eps4[a * nt + t] = F(4 * e);
+            B->site_sigma[a * nt + t] = sg;
+            B->site_eps[a * nt + t] = e;
+        }
+    }
+    pa::DevBatch<F>& d = view<F>(B);
+    cudaStream_t st = ctx->stream;
+    PA_CUDA(ctx, cudaMemcpyAsync(const_cast<F*>(d.sig2), sig2.data(), sizeof(F) * sig2.size(), cudaMemcpyHostToDevice, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(const_cast<F*>(d.eps4), eps4.data(), sizeof(F) * eps4.size(), cudaMemcpyHostToDevice, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(d.const_offset), constant_offset, sizeof(double) * B->nfw,
+                                 cudaMemcpyHostToDevice, st));
+    return wait_stream(ctx);
+}
+
 }  // namespace
 
 extern "C" {
@@ -666,6 +699,15 @@ pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t pr
     B->nsys = desc->nsys; B->nfw = nfw; B->ntypes = desc->ntypes; B->nguest = desc->nguest;
     B->natoms = na; B->nk = nk;
     B->framework_of.assign(desc->framework_of, desc->framework_of + desc->nsys);
+    for (int a = 0; a < desc->nguest; ++a) {
+        B->guest_types.push_back(desc->guest_types[a] - 1);
+        B->guest_q.push_back(desc->guest_charges[a]);
+    }
+    B->cutoff = desc->cutoff;
+    B->recip_bound.assign(nfw, 0.0);
+    for (int f = 0; f < nfw; ++f)
+        for (int32_t i = desc->k_offsets[f]; i < desc->k_offsets[f + 1]; ++i)
+            B->recip_bound[f] += desc->kprefactor[i] * std::hypot(desc->Shost[2 * i], desc->Shost[2 * i + 1]);
     B->atom_offsets.assign(desc->atom_offsets, desc->atom_offsets + nfw + 1);
     B->k_offsets.assign(desc->k_offsets, desc->k_offsets + nfw + 1);
     pa_status st = precision == PA_PRECISION_F32 ? upload_impl<float>(ctx, desc, B) : upload_impl<double>(ctx, desc, B);
@@ -686,6 +728,53 @@ pa_status pa_batch_free(pa_batch* batch) {
     cudaSetDevice(batch->device);
     cudaDeviceSynchronize();
     delete batch;
+    return PA_OK;
+}
+
+pa_status pa_batch_set_pair_tables(pa_context* ctx, pa_batch* B, const double* sigma, const double* epsilon,
+                                   const double* constant_offset) {
+    if (!ctx || !B || !sigma || !epsilon || !constant_offset) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    return B->precision == PA_PRECISION_F32 ? set_pair_tables_impl<float>(ctx, B, sigma, epsilon, constant_offset)
+                                            : set_pair_tables_impl<double>(ctx, B, sigma, epsilon, constant_offset);
+}
+
+pa_status pa_batch_hardcore_bounds(pa_context* ctx, const pa_batch* B, double* bs) {
+    if (!ctx || !B || !bs) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    const int N = B->nguest, nt = B->ntypes, nfw = B->nfw;
+    // [site sigma N*nt][site eps N*nt][guest charges N][bounds nfw][error flag]
+    std::vector<double> h(2 * N * nt + N + nfw + 1, 0.0);
+    std::copy(B->site_sigma.begin(), B->site_sigma.end(), h.begin());
+    std::copy(B->site_eps.begin(), B->site_eps.end(), h.begin() + N * nt);
+    std::copy(B->guest_q.begin(), B->guest_q.end(), h.begin() + 2 * N * nt);
+    cudaStream_t st = ctx->stream;
+    PA_CUDA(ctx, ctx->bnd.ensure(sizeof(double) * h.size()));
+    PA_CUDA(ctx, cudaMemcpyAsync(ctx->bnd.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+    double* d = ctx->bnd.as<double>();
+    const pa::DevBatch<float>& v32 = B->d32;
+    const pa::DevBatch<double>& v64 = B->d64;
+    pa::BoundArgs g{};
+    g.types = B->types0; g.charges = B->q64;
+    g.atom_offsets = B->precision == PA_PRECISION_F32 ? v32.atom_offsets : v64.atom_offsets;
+    g.alphas = B->precision == PA_PRECISION_F32 ? v32.alphas : v64.alphas;
+    g.site_sig = d; g.site_eps = d + N * nt; g.gq = d + 2 * N * nt; g.N = N; g.nt = nt; g.r_lj = B->cutoff;
+    g.out = d + 2 * N * nt + N;
+    g.err = reinterpret_cast<int32_t*>(d + 2 * N * nt + N + nfw);
+    pa::k_hardcore_bound<<<unsigned(nfw), 256, 0, st>>>(g);
+    PA_CUDA(ctx, cudaGetLastError());
+    std::vector<double> out(nfw + 1);
+    PA_CUDA(ctx, cudaMemcpyAsync(out.data(), g.out, sizeof(double) * (nfw + 1), cudaMemcpyDeviceToHost, st));
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    int32_t e = 0;
+    std::memcpy(&e, &out[nfw], sizeof(int32_t));
+    if (e) return fail(ctx, PA_ERR_ARG, "hard-core bound: a root search (find_r0) failed");
+    double qabs = 0;
+    for (double q : B->guest_q) qabs += std::fabs(q);
+    for (int f = 0; f < nfw; ++f) bs[f] = out[f] + 2 * pa::KE * qabs * B->recip_bound[f];
     return PA_OK;
 }
 

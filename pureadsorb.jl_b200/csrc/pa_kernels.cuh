@@ -631,4 +631,85 @@ __global__ void __launch_bounds__(256) k_structure_factor(const double* ks, int6
     if (i < nk) { S[2 * i] = re; S[2 * i + 1] = im; }
 }
 
+// ---------------------------------------------------------------------------------------------
+// k_hardcore_bound: the hard-core bound B_s of each framework on the device (src/reject.jl:95-124,
+// the reference's `hardcore_bound`): Σ over guest sites a and host atoms j of eps_aj for repulsive
+// or neutral pairs, and eps_aj + |K| erfc(alpha r0)/r0 for attractive ones (K = KE q_a q_j < 0),
+// r0 the zero of LJ + screened Coulomb below the LJ minimum (find_r0, src/reject.jl:46-69,
+// bisection to 4 eps relative, clamped to r_lj). FP64. One CTA per framework, a fixed-order
+// reduction; err[0] gets 1 when a bracket search fails and B_s is +inf for an attractive pair
+// without an LJ wall.
+// ---------------------------------------------------------------------------------------------
+struct BoundArgs {
+    const int32_t* types;    // natoms, 0-based compact
+    const double* charges;   // natoms
+    const int32_t* atom_offsets;
+    const double* alphas;    // nfw
+    const double* site_sig;  // N*nt (site, type)
+    const double* site_eps;  // N*nt
+    const double* gq;        // N guest charges
+    int32_t N, nt;
+    double r_lj;
+    double* out;             // nfw
+    int32_t* err;
+};
+
+__device__ __forceinline__ double bound_pair_energy(double r, double s, double e, double K, double alpha) {
+    double x = (s * s) / (r * r);
+    x = x * x * x;
+    return 4.0 * e * (x * x - x) + K * erfc(alpha * r) / r;
+}
+
+__device__ double bound_find_r0(double s, double e, double K, double alpha, double r_lj, int32_t* err) {
+    double hi = s * 1.122462048309373;  // 2^(1/6)
+    if (!(bound_pair_energy(hi, s, e, K, alpha) < 0)) { *err = 1; return r_lj; }
+    double lo = hi;
+    int it = 0;
+    while (bound_pair_energy(lo, s, e, K, alpha) <= 0) {
+        lo *= 0.5;
+        if (++it > 200) { *err = 1; return r_lj; }
+    }
+    it = 0;
+    const double eps = 2.220446049250313e-16;
+    while (hi - lo > 4 * eps * hi) {
+        const double mid = (lo + hi) / 2;
+        if (bound_pair_energy(mid, s, e, K, alpha) > 0) lo = mid; else hi = mid;
+        if (++it > 200) { *err = 1; return r_lj; }
+    }
+    return fmin((lo + hi) / 2, r_lj);
+}
+
+__global__ void __launch_bounds__(256) k_hardcore_bound(BoundArgs g) {
+    __shared__ double s_red[256];
+    const int32_t fw = blockIdx.x;
+    const int32_t a0 = g.atom_offsets[fw], a1 = g.atom_offsets[fw + 1];
+    const double alpha = g.alphas[fw];
+    const int64_t npair = int64_t(a1 - a0) * g.N;
+    double acc = 0.0;
+    int32_t lerr = 0;
+    for (int64_t p = threadIdx.x; p < npair; p += blockDim.x) {
+        const int32_t a = int32_t(p / (a1 - a0)), j = a0 + int32_t(p % (a1 - a0));
+        const int32_t t = g.types[j];
+        const double e = g.site_eps[a * g.nt + t], s = g.site_sig[a * g.nt + t];
+        const double K = KE * g.gq[a] * g.charges[j];
+        double term = e;
+        if (K < 0) {
+            if (e == 0) term = __longlong_as_double(0x7ff0000000000000LL);
+            else {
+                const double r0 = bound_find_r0(s, e, K, alpha, g.r_lj, &lerr);
+                term = e + fabs(K) * erfc(alpha * r0) / r0;
+            }
+        }
+        acc += term;
+    }
+    if (lerr) atomicExch(g.err, 1);
+    s_red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (int(threadIdx.x) < w) s_red[threadIdx.x] += s_red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) g.out[fw] = s_red[0];
+}
+
 }  // namespace pa

@@ -78,27 +78,40 @@ def hardcore_bound(guest_types, guest_charges, sigma, epsilon, types, charges, r
     """B_s: lower-magnitude bound on every pair's energy plus the reciprocal cross-term bound,
     Inf when a pair is attractive with no LJ wall (src/reject.jl:95-124). Types are 1-based
     indices into sigma/epsilon."""
-    acc = 0.0
+    ht = np.asarray(types, dtype=np.int64) - 1
+    q = np.asarray(charges, dtype=np.float64)
+    # per site: the attractive pairs' (sigma, eps, K) triples; sigma and eps depend only on the
+    # host type, so the distinct triples are (type, distinct K). One bisection per distinct triple
+    # (as the reference memoises), all of a framework's triples in one vectorised call.
+    sites, groups, ss, es, ks = [], [], [], [], []
     for a in range(len(guest_types)):
         gt = int(guest_types[a]) - 1
-        qa = float(guest_charges[a])
-        ht = np.asarray(types, dtype=np.int64) - 1
-        sg = sigma[gt, ht]
         ep = epsilon[gt, ht]
-        K = KE * qa * np.asarray(charges, dtype=np.float64)
+        K = KE * float(guest_charges[a]) * q
         att = K < 0
         if np.any(att & (ep == 0)):
             return math.inf
+        sites.append((ep, att))
+        for t in np.unique(ht[att]):
+            sel = att & (ht == t)
+            uk, inv = np.unique(K[sel], return_inverse=True)
+            groups.append((a, sel, inv.reshape(-1), sum(len(x) for x in ks), len(uk), float(epsilon[gt, t])))
+            ss.append(np.full(len(uk), float(sigma[gt, t])))
+            es.append(np.full(len(uk), float(epsilon[gt, t])))
+            ks.append(uk)
+    bound = None
+    if ks:
+        uk_all = np.concatenate(ks)
+        r0 = find_r0(np.concatenate(ss), np.concatenate(es), uk_all, alpha, r_lj)
+        bound = np.concatenate(es) + np.abs(uk_all) * erfc(alpha * r0) / r0
+    acc = 0.0
+    for a, (ep, att) in enumerate(sites):
         terms = ep.copy()
-        if np.any(att):
-            # one bisection per distinct (sigma, eps, K) triple, as the reference memoises
-            trip = np.stack([sg[att], ep[att], K[att]], axis=1)
-            uniq, inv = np.unique(trip, axis=0, return_inverse=True)
-            r0 = find_r0(uniq[:, 0], uniq[:, 1], uniq[:, 2], alpha, r_lj)
-            bound = uniq[:, 1] + np.abs(uniq[:, 2]) * erfc(alpha * r0) / r0
-            terms[att] = bound[inv.reshape(-1)]
-        for v in terms:  # sequential sum in atom order
-            acc += float(v)
+        for ga, sel, inv, o, n, e_t in groups:
+            if ga == a:
+                terms[sel] = bound[o:o + n][inv]
+        # sequential sum in atom order (builtin sum() of floats compensates, so accumulate)
+        acc = float(np.add.accumulate(np.concatenate(([acc], terms)))[-1])
     Rs = 0.0
     for i in range(len(kprefactor)):
         Rs += float(kprefactor[i]) * abs(complex(Shost[i]))

@@ -14,6 +14,8 @@ frameworks generated deterministically from numpy's PCG64 (numpy.random.default_
             when degenerate), log-uniform 50..2000 atoms per unit cell, 3..6 own types each with
             eps/kB U(15,80) K and sigma U(2.3,3.6) A, zero-sum N(0, 0.5 e) charges, uniform
             positions, replicated until every perpendicular width reaches 2 (rc + r_guest).
+- fitting:  nfw frameworks (seed 11) drawn like `batched` but typed from one shared 4-type palette,
+            plus 8 hidden scale factors U(0.9, 1.1) of the palette's (epsilon, sigma).
 """
 import math
 
@@ -89,21 +91,27 @@ def co2(T=np.float64, seed=42, replication=(3, 3, 3)):
                                                                                      seed=42, nblocks=10)
 
 
+def _geometry(rng, max_unit_atoms):
+    """One framework's cell and atom count as the batched workload draws them."""
+    while True:
+        L = rng.uniform(8.0, 30.0, 3)
+        ang = rng.uniform(60.0, 120.0, 3)
+        try:
+            A = cell_matrix(L[0], L[1], L[2], ang[0], ang[1], ang[2])
+            break
+        except ArgumentError:
+            continue
+    na = int(round(math.exp(rng.uniform(math.log(50), math.log(max_unit_atoms)))))
+    return A, na
+
+
 def batched(nfw=64, seed=7, T=np.float64, max_unit_atoms=2000):
     """The batched uneven-framework workload: nfw distinct frameworks."""
     rng = np.random.default_rng(seed)
     rc, r_guest = 12.0, 1.16
     fws, names, sig, eps = [], [], [], []
     for n in range(nfw):
-        while True:
-            L = rng.uniform(8.0, 30.0, 3)
-            ang = rng.uniform(60.0, 120.0, 3)
-            try:
-                A = cell_matrix(L[0], L[1], L[2], ang[0], ang[1], ang[2])
-                break
-            except ArgumentError:
-                continue
-        na = int(round(math.exp(rng.uniform(math.log(50), math.log(max_unit_atoms)))))
+        A, na = _geometry(rng, max_unit_atoms)
         nt = int(rng.integers(3, 7))
         tnames = [f"F{n}T{t}" for t in range(nt)]
         names += [x + "_" for x in tnames]
@@ -121,3 +129,35 @@ def batched(nfw=64, seed=7, T=np.float64, max_unit_atoms=2000):
     ff = ForceField(names, sig, eps, cutoff=rc, tail=True)
     return fws, ff, co2_guest(ff), EwaldParams(cutoff=rc, precision=1.0e-6), dict(T=298.15, ninsert=nfw * 2**20,
                                                                                   seed=7, nblocks=10)
+
+
+PALETTE = ("P0", "P1", "P2", "P3")
+
+
+def fitting(nfw=128, seed=11, T=np.float64, max_unit_atoms=2000):
+    """The force-field fitting workload: nfw frameworks drawn like the batched workload (cells,
+    atom counts, uniform positions, zero-sum N(0, 0.5 e) charges, replication) whose atoms share
+    one 4-type host palette P0..P3 (round-robin), so that the fitted parameters are the palette's
+    4 x (epsilon, sigma). The palette's eps/kB U(15,80) K and sigma U(2.3,3.6) A come first from
+    the seeded stream; after the frameworks, 8 hidden scale factors U(0.9, 1.1) (epsilon of P0..P3,
+    then sigma of P0..P3) define the parameters the targets are computed at."""
+    rng = np.random.default_rng(seed)
+    rc, r_guest = 12.0, 1.16
+    pal_eps = rng.uniform(15.0, 80.0, 4) * KB
+    pal_sig = rng.uniform(2.3, 3.6, 4)
+    fws = []
+    for n in range(nfw):
+        A, na = _geometry(rng, max_unit_atoms)
+        frac = rng.random((na, 3))
+        q = rng.normal(0.0, 0.5, na)
+        q -= q.mean()
+        symbols = [PALETTE[i % 4] for i in range(na)]
+        unit = Framework(A, frac, symbols, symbols, q, (1, 1, 1), T)
+        fws.append(replicate(unit, min_multiplicity(A, rc + r_guest)))
+    hidden = rng.uniform(0.9, 1.1, 8)
+    names = [p + "_" for p in PALETTE] + [t[0] for t in CO2_TYPES]
+    ff = ForceField(names, list(pal_sig) + [t[1] for t in CO2_TYPES], list(pal_eps) + [t[2] * KB for t in CO2_TYPES],
+                    cutoff=rc, tail=True)
+    return fws, ff, co2_guest(ff), EwaldParams(cutoff=rc, precision=1.0e-6), dict(
+        T=298.15, ninsert_per_framework=2**18, seed=seed, nblocks=10, steps=200, lr=1e-2, hidden=hidden,
+        fitted_types=[p + "_" for p in PALETTE])

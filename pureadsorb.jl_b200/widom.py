@@ -222,6 +222,16 @@ def block_sums(lse, sw, suw):
         return scale * sw, scale * suw
 
 
+def lnkh_from_sums(batch, kT, nblocks, lse, sw, suw, cnt):
+    """ln K_H = ln(V <W> / kT) of every system from a call's raw block sums, -inf for a system
+    whose every weight is zero (no accessible volume), where widom's reduction throws."""
+    sW, _ = block_sums(lse, sw, suw)
+    W = sW.reshape(batch.nsys, nblocks).sum(axis=1) / np.asarray(cnt).reshape(batch.nsys, nblocks).sum(axis=1)
+    Vf = batch.volumes.astype(batch.T).astype(np.float64)[np.asarray(batch.framework_of, dtype=np.int64) - 1]
+    with np.errstate(divide="ignore"):
+        return np.log(Vf) + np.log(W) - math.log(float(kT))
+
+
 def _results(batch, kT, nblocks, lse, sw, suw, cnt):
     sW, sUW = block_sums(lse, sw, suw)
     sW = sW.reshape(batch.nsys, nblocks)

@@ -1,0 +1,75 @@
+"""The batched workload on the B200: 64 uneven frameworks (348,897 stored atoms, 283 LJ types,
+33,096 coupled k-vectors) in one call, against the FP64 oracle at the same FP32 poses: poses and
+phase-0 flags exact, per-insertion ΔU within the FP32 tolerance, and per framework
+|Δ ln K_H| <= 1e-3 and |Δ q_st| <= 5.18e-4 eV (0.05 kJ/mol). The same comparison against the plain
+FP64 device form also carries the F32-vs-F64 pose rounding (the two forms draw the same uniforms
+at 24 and 53 bits), which alone moves ln K_H of the most sensitive framework by about 1e-3 at
+2^14 insertions per framework.
+
+These frameworks have no minimum atom separation, so some insertions sum large screened-Coulomb
+terms of both signs; the FP32 rounding of those terms (not of their compensated sum) can then
+exceed the parity tolerance slightly. The test allows that for at most 1 in 10^4 survivors, within
+twice the tolerance."""
+import numpy as np
+import pytest
+
+from conftest import kT_of, oracle_view
+from test_gpu_parity import F32_ABS, F32_REL
+
+
+def orc_counts(n, nsys, run):
+    q, rem = divmod(n, run)
+    full, hi = divmod(q, nsys)
+    ns = [full * run] * nsys
+    for r in range(hi):
+        ns[r] += run
+    if rem > 0:
+        ns[q % nsys] += rem
+    return ns
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batched_frameworks_against_oracle_same_poses(pa, orc, backend):
+    fws, ff, guest, ewald, prm = pa.synthetic.batched(T=np.float32)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, sk=backend.ctx.structure_factor)
+    n, nb = len(fws) * 2**12, 10
+    run = pa.default_run(n, len(fws))
+    ins = {}
+    lse, sw, suw, cnt = pa._widom(b, guest, reject=True, T=298.15, ninsert=n, seed=7, nblocks=nb, backend=backend,
+                                  insertions=ins, segment_range=(0, 0))
+    kT = kT_of(pa, b)
+    v, keep = oracle_view(orc, b)
+    rho2, reach0 = pa.build_rejection_tables(b, kT)
+    ref = orc.widom(v, 32, kT, n, 7, nb, run, True, rho2, reach0)
+    assert np.array_equal(ins["poses"], ref["poses"])
+    assert np.array_equal(ins["flags"], ref["flags"])
+    surv = ref["flags"] == 0
+    a, r = ins["dU"][surv], ref["dU"][surv]
+    bad = np.abs(a - r) > F32_ABS + F32_REL * np.abs(r)
+    sysid = np.repeat(np.arange(len(fws)), np.asarray(orc_counts(n, len(fws), run)))[surv]
+    x = -r / kT
+    xmax = np.full(len(fws), -np.inf)
+    np.maximum.at(xmax, sysid, x)
+    heavy = x >= xmax[sysid] - 50
+    o = np.argsort(-np.abs(a - r))[:8]
+    print(f"\nper-insertion: {int(bad.sum())} of {len(r)} survivors outside the tolerance, {int((bad & heavy).sum())} of "
+          f"{int(heavy.sum())} heavy; worst (ref dU, dev - ref, heavy): "
+          + ", ".join(f"({r[i]:.4g}, {a[i] - r[i]:.2e}, {bool(heavy[i])})" for i in o)
+          + "; outside: " + ", ".join(f"({r[i]:.6g}, {a[i] - r[i]:.3e}, x-xmax={x[i] - xmax[sysid[i]]:.2f})"
+                                      for i in np.nonzero(bad)[0][:8]))
+    sW, sUW = pa.block_sums(lse, sw, suw)
+    W = sW.reshape(len(fws), nb).sum(axis=1)
+    UW = sUW.reshape(len(fws), nb).sum(axis=1)
+    Wr, UWr = ref["sW"].sum(axis=1), ref["sUW"].sum(axis=1)
+    assert np.array_equal(W > 0, Wr > 0)
+    ok = Wr > 0
+    dln = np.abs(np.log(W[ok]) - np.log(Wr[ok]))
+    dq = np.abs(UW[ok] / W[ok] - UWr[ok] / Wr[ok])
+    print(f"\nbatched: {int(ok.sum())} frameworks with accessible volume, max |d ln K_H| {dln.max():.2e}, "
+          f"max |d q_st| {dq.max():.2e} eV")
+    assert dln.max() <= 1e-3
+    assert dq.max() <= 5.18e-4
+    assert bad.sum() <= 1e-4 * len(r)
+    assert np.all(np.abs(a - r) <= 2 * (F32_ABS + F32_REL * np.abs(r)))
+    b.drop_device()
