@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-fit", action="store_true")
+    p.add_argument("--no-tune", action="store_true", help="default bin width and grid (e.g. for profiling)")
     return p.parse_args()
 
 
@@ -303,8 +304,11 @@ def main():
 
     # layout and launch shape chosen by the autotuner on this rank's own call, then every step
     # replayed from a CUDA graph
-    tune = pa.autotune(batch, guest, T=prm["T"], ninsert=args.ninsert, backend=backend, seed=prm["seed"],
-                       nblocks=nblocks)
+    if args.no_tune:
+        tune = pa.TuneReport(3.0, 8, float("nan"), [])
+    else:
+        tune = pa.autotune(batch, guest, T=prm["T"], ninsert=args.ninsert, backend=backend, seed=prm["seed"],
+                           nblocks=nblocks)
     ctx.set_tuning(use_graphs=True)
     for _ in range(max(3, args.warmup)):
         step()
