@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
 #pragma unroll
         for (int s = 0; s < NS; ++s) { sg[s] = 0.f; ep[s] = 0.f; }
         const float NLOG2E = -1.4426950408889634f;
+        const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
         // tmo_at: chunk whose copy did not arrive in time (-1: none); after it no copies are issued
         // and only the chunk already in flight is still waited for
         int32_t tmo_at = -1;
@@ -141,6 +142,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
 #pragma unroll
                         for (int s = 0; s < NS; ++s) { sg[s] = s_sig2[s * nt + ty]; ep[s] = s_eps4[s * nt + ty]; }
                     }
+                    // the entry's site terms are summed plainly (at most NS of them), and that sum
+                    // enters the compensated per-insertion sum once per entry
+                    float ee = 0.f;
 #pragma unroll
                     for (int s = 0; s < NS; ++s) {
                         const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
@@ -163,16 +167,17 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                     float p = cf[PA_NERFC32 - 1];
 #pragma unroll
                                     for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
-                                    e = fmaf(gqk[s] * at.w, p * ex2_ftz((z * z) * NLOG2E) * ri, e);
+                                    e = fmaf(gqk[s] * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
                                 }
                             } else {
                                 const float x = sg[s] * rcp_nr(r2);
                                 const float x3 = x * x * x;
                                 e = ep[s] * (x3 * x3 - x3);
                             }
-                            kahan_add(esum, ecmp, e);
+                            ee += e;
                         }
                     }
+                    kahan_add(esum, ecmp, ee);
                 }
             }
             __syncwarp();  // the warp is done with stage st
