@@ -92,15 +92,12 @@ def fold_replicas(g, natoms_unit):
     return g.reshape(-1, natoms_unit).sum(axis=0)
 
 
-def widom_grad(batch, guest, ff, *, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None,
-               window=0.0, reduce=True):
-    """widom plus d ln K_H / dθ for every system: returns (results, grads), grads[s] a WidomGrad.
-    θ: the per-type LJ ε and σ of `ff` (which must be the force field the batch was built from)
-    and the charges of each framework's atoms. The batch must be FP32 (the adjoint walks the FP32
-    path's neighbour lists). Insertions whose weight is below exp(-window) times their system's
-    largest are left out of the sums (0 selects 50). With reduce=False the first element is
-    ln K_H per system from the raw sums instead of the WidomResults (-inf, and NaN gradients,
-    for a system without accessible volume, where the reduction throws)."""
+def grad_sums(batch, guest, *, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None, window=0.0,
+              segment_range=(0, 0), segments_out=None):
+    """One pa_widom_grad call. Returns (kT, (lse, sw, suw, cnt), sums): the call's raw block sums
+    and, per system, a dict of its adjoint sums (xmax, sum_w, d_epsilon and d_sigma per (site,
+    compact type), d_charge per stored atom, recomputed). segment_range restricts the call to a
+    shard of the job (see combine_sums)."""
     nsys = batch.nsys
     N = len(batch.guest_types)
     nt = len(batch.sigma)
@@ -111,15 +108,42 @@ def widom_grad(batch, guest, ff, *, T, ninsert, backend=None, seed=0, chunk=2**1
                        _lib.ptr(buf["d_sigma"]), _lib.ptr(buf["d_charge"]), None, float(window), 0)
     T = float(T.magnitude) if hasattr(T, "magnitude") else float(T)
     kT = float(batch.T(KB * T))
-    lse, sw, suw, cnt = _widom(batch, guest, reject=True, T=T, ninsert=ninsert, backend=backend, seed=seed,
-                               chunk=chunk, nblocks=nblocks, run=run, segment_range=(0, 0), grad_sums=gs)
+    raw = _widom(batch, guest, reject=True, T=T, ninsert=ninsert, backend=backend, seed=seed, chunk=chunk,
+                 nblocks=nblocks, run=run, segment_range=segment_range, segments_out=segments_out, grad_sums=gs)
+    aoff = np.concatenate([[0], np.cumsum(nat)]).astype(np.int64)
+    sums = [dict(xmax=buf["xmax"][s], sum_w=buf["sum_w"][s], d_epsilon=buf["d_epsilon"].reshape(nsys, N, nt)[s],
+                 d_sigma=buf["d_sigma"].reshape(nsys, N, nt)[s], d_charge=buf["d_charge"][aoff[s]:aoff[s + 1]],
+                 recomputed=gs.recomputed) for s in range(nsys)]
+    return kT, raw, sums
+
+
+def combine_sums(shards):
+    """One system's adjoint sums of a whole job from the sums of disjoint shards of it (several
+    GPUs, each with its own segment range and so its own shift xmax): every shard is rescaled to
+    the largest shift and the shards are added in the given order."""
+    xm = max(float(p["xmax"]) for p in shards)
+    out = dict(xmax=xm, recomputed=sum(int(p.get("recomputed", 0)) for p in shards))
+    for k in ("sum_w", "d_epsilon", "d_sigma", "d_charge"):
+        acc = None
+        for p in shards:
+            f = math.exp(float(p["xmax"]) - xm) if np.isfinite(p["xmax"]) else 0.0
+            v = f * np.asarray(p[k], dtype=np.float64)
+            acc = v if acc is None else acc + v
+        out[k] = acc
+    return out
+
+
+def widom_grad(batch, guest, ff, *, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None,
+               window=0.0, reduce=True):
+    """widom plus d ln K_H / dθ for every system: returns (results, grads), grads[s] a WidomGrad.
+    θ: the per-type LJ ε and σ of `ff` (which must be the force field the batch was built from)
+    and the charges of each framework's atoms. The batch must be FP32 (the adjoint walks the FP32
+    path's neighbour lists). Insertions whose weight is below exp(-window) times their system's
+    largest are left out of the sums (0 selects 50). With reduce=False the first element is
+    ln K_H per system from the raw sums instead of the WidomResults (-inf, and NaN gradients,
+    for a system without accessible volume, where the reduction throws)."""
+    kT, (lse, sw, suw, cnt), sums = grad_sums(batch, guest, T=T, ninsert=ninsert, backend=backend, seed=seed,
+                                              chunk=chunk, nblocks=nblocks, run=run, window=window)
     results = _results(batch, kT, nblocks, lse, sw, suw, cnt) if reduce else \
         lnkh_from_sums(batch, kT, nblocks, lse, sw, suw, cnt)
-    aoff = np.concatenate([[0], np.cumsum(nat)]).astype(np.int64)
-    grads = []
-    for s in range(nsys):
-        sums = dict(xmax=buf["xmax"][s], sum_w=buf["sum_w"][s],
-                    d_epsilon=buf["d_epsilon"].reshape(nsys, N, nt)[s], d_sigma=buf["d_sigma"].reshape(nsys, N, nt)[s],
-                    d_charge=buf["d_charge"][aoff[s]:aoff[s + 1]], recomputed=gs.recomputed)
-        grads.append(assemble(batch, ff, s, sums, kT))
-    return results, grads
+    return results, [assemble(batch, ff, s, sums[s], kT) for s in range(batch.nsys)]

@@ -109,3 +109,60 @@ def test_two_rank_shards_combine_exactly(tmp_path):
     np.testing.assert_allclose(sW, ref["sW"].reshape(-1), rtol=1e-12)
     np.testing.assert_allclose(sUW, ref["sUW"].reshape(-1), rtol=1e-10, atol=1e-300)
     assert np.array_equal(a[3], ref["n"].reshape(-1))
+
+
+def grad_worker(rank, world, port, outdir):
+    """Each rank takes the adjoint sums of its own half of the job's insertions (the rest masked
+    as rejected, which carries zero weight), with its own shift; rank 0 combines the gathered
+    shards."""
+    import pickle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        pa, batch, kT, run, ref = job()
+        v, keep = pa_oracle_view(batch)
+        flags = ref["flags"].copy()
+        lo, hi = NINSERT * rank // world, NINSERT * (rank + 1) // world
+        flags[:lo] = 1
+        flags[hi:] = 1
+        mine = grad_sums_oracle(pa, batch, kT, run, dict(ref, flags=flags))
+        shards = [None] * world
+        dist.all_gather_object(shards, mine)
+        if rank == 0:
+            combined = [pa.adjoint.combine_sums([shards[r][s] for r in range(world)]) for s in range(batch.nsys)]
+            with open(os.path.join(outdir, "grad.pkl"), "wb") as fh:
+                pickle.dump(combined, fh)
+    finally:
+        dist.destroy_process_group()
+
+
+def pa_oracle_view(batch):
+    import sys
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    orc = ge.load_oracle()
+    return orc.view(batch, batch.guest_sites_orig, batch.guest_charges_orig, batch.cutoff, batch.ewald_cutoff)
+
+
+def grad_sums_oracle(pa, batch, kT, run, out):
+    import sys
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    orc = ge.load_oracle()
+    v, keep = pa_oracle_view(batch)
+    nat, nk = pa.adjoint.system_offsets(batch)
+    return orc.grad_sums(v, kT, NINSERT, run, out, nat, nk)
+
+
+def test_two_rank_adjoint_shards_combine(tmp_path):
+    import pickle
+    world = 2
+    mp.spawn(grad_worker, args=(world, free_port(), str(tmp_path)), nprocs=world, join=True)
+    with open(tmp_path / "grad.pkl", "rb") as fh:
+        combined = pickle.load(fh)
+    pa, batch, kT, run, ref = job()
+    full = grad_sums_oracle(pa, batch, kT, run, ref)
+    for s in range(batch.nsys):
+        assert combined[s]["xmax"] == full[s]["xmax"]
+        for k in ("sum_w", "d_epsilon", "d_sigma", "d_charge"):
+            np.testing.assert_allclose(combined[s][k], full[s][k], rtol=1e-12, atol=1e-14 * np.max(np.abs(full[s][k])))
