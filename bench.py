@@ -373,10 +373,12 @@ def main():
         kc = batch.kcoeffs
         rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
         # executed FP32 work of k_energy32 per survivor (FMA = 2 flops; model stated in DESIGN.md):
-        # 8 per (list entry, site) distance, 52 per in-cutoff pair (LJ 10 + screened Coulomb 38 +
-        # compensated add 4), 10 per (k, site) + 7 per k for the reciprocal recurrence, 25 per
-        # (row start, site) for the direct phase evaluation
-        flops_surv = 8 * N * L + 52 * n_lj + (10 * N + 7) * nk + 25 * N * rows
+        # each of its N (insertion, site) items walks its bin's list, 8 flops per entry for the
+        # distance, and 52 per in-cutoff pair (LJ 10 + screened Coulomb 38 + compensated add 4).
+        # The reciprocal term (k_recip32: 10 per (k, site) + 7 per k for the recurrence, 25 per
+        # (row start, site)) runs in its own kernel and is reported beside it.
+        flops_surv = 8 * N * L + 52 * n_lj
+        flops_recip = (10 * N + 7) * nk + 25 * N * rows
         e_ms = kms[2] / max(1, kn[2])
         surv_per_launch = surv_frac * (s1 - s0) * (ninsert / nseg)
         achieved = flops_surv * surv_per_launch / (e_ms / 1e3) / 1e12
@@ -386,7 +388,8 @@ def main():
                 "traffic": ENERGY32_TRAFFIC_BYTES if args.ninsert == 1_000_000 and world == 1 else None,
                 "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
                 "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
-                "flops_per_survivor": flops_surv, "reference_algorithm_flops_per_survivor": ref_alg,
+                "flops_per_survivor": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
+                "reciprocal_combine_ms_per_step": kms[6] / args.steps, "reference_algorithm_flops_per_survivor": ref_alg,
                 "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew}
 
         # plain FP64 form on the same workload and stream (the >= 3x denominator)
@@ -477,9 +480,10 @@ def main():
                 "clocks": clk.summary(),
                 "tuning": {"bin_width": tune.bin_width, "ctas_per_sm": tune.ctas_per_sm, "cuda_graphs": True,
                            "candidates": [list(r) for r in tune.table]},
-                "gpu_launches": int(5 * args.steps),
+                "gpu_launches": int(9 * args.steps),
                 "kernel_ms": {"pose_phase0": kms[0] / args.steps, "scan_scatter": kms[1] / args.steps,
-                              "energy": kms[2] / args.steps, "segment_reduce": kms[3] / args.steps},
+                              "energy": kms[2] / args.steps, "reciprocal_combine": kms[6] / args.steps,
+                              "segment_reduce": kms[3] / args.steps},
                 "roofline": roof,
                 "fp64_plain": fp64,
                 "adjoint": adj,

@@ -56,9 +56,10 @@ const char* pa_last_error(const pa_context* ctx);
 /* Enables per-kernel CUDA-event timing inside pa_widom (adds events, no synchronisation). */
 pa_status pa_context_set_timing(pa_context* ctx, int32_t enable);
 /* Total device milliseconds and launch counts per kernel class since timing was enabled.
- * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy, 3 reduction, 4 neighbour-list build,
- * 5 adjoint (selection, recomputation, reciprocal charge term). */
-pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*6*/, int64_t* launches /*6*/);
+ * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy (real space), 3 reduction, 4 neighbour-list
+ * build, 5 adjoint (selection, recomputation, reciprocal charge term), 6 FP32 reciprocal term and
+ * per-insertion sum. */
+pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*7*/, int64_t* launches /*7*/);
 
 /* Layout and launch choices of a context (no counterpart in the reference), set by the
  * autotuner or by hand. bin_width: edge in Å of the FP32 path's spatial bins, applied to batches
@@ -209,9 +210,10 @@ pa_status pa_rejection_tables(const pa_batch_desc* desc, const double* bs, const
  * not allocate device memory during the call (a host application that owns a fixed memory
  * budget, strict per-tenant accounting, or code that must avoid cudaMalloc's device-wide
  * synchronisation): the same kernels as pa_widom, with every per-call scratch buffer carved out
- * of one file-scope device array of 16 MiB that each GPU loading the library holds until the
- * process exits. Limits: at most 131,072 insertions per call, 1,024 systems, 32,768 spatial bins
- * and 65,536 rejection radii; larger calls return PA_ERR_ARG. Only per_insertion->dU may be
+ * of one file-scope device array of 32 MiB that each GPU loading the library holds until the
+ * process exits. Limits: at most 131,072 insertions per call (and, for an FP32 batch, 393,216
+ * insertion-site pairs), 1,024 systems, 32,768 spatial bins and 65,536 rejection radii; larger
+ * calls return PA_ERR_ARG. Only per_insertion->dU may be
  * requested. All calls share the array (host calls are serialised by a mutex); device work of two
  * calls must not overlap. The first call on a device looks up the array's address and should
  * come before any stream capture. */

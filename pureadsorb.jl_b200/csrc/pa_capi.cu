@@ -21,7 +21,7 @@ static_assert(PA_SEGMENT_SIZE == PA_SEGMENT, "segment size mismatch");
 
 namespace {
 
-constexpr int NCLASS = 6;  // kernel classes for timing: pose, scan/scatter, energy, reduce, lists, adjoint
+constexpr int NCLASS = 7;  // kernel classes: pose, scan/scatter, energy, reduce, lists, adjoint, reciprocal+combine
 constexpr double LIST_PAD = 32;
 constexpr double DEFAULT_BIN_WIDTH = 3.0;  // Angstrom, FP32 path spatial bins
 constexpr double WAIT_LIMIT_S = 600.0;      // host-side bound on one call's device work
@@ -56,6 +56,8 @@ struct pa_context {
     // per-call workspace (grow-only)
     DevMem pose_a, pose_b, bin_of, slot, sorted, dU, bin_count, fine_start, bin_start, tile_start, counters, seg_out, seg_rng,
         sys_off, rho2, reach0;
+    // FP32 path: (insertion, site) work items
+    DevMem item_bin, item_slot, item_sorted, item_count, item_fine_start, item_bin_start, item_tile_start, dUs, dUr;
     // adjoint workspace
     DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
     // launch choices, the replayable graph of the last call's device sequence and its key
@@ -550,6 +552,15 @@ cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Wor
     return cudaGetLastError();
 }
 
+// The FP32 path's reciprocal term (charged guests) and the per-insertion sum of the site terms.
+template <int NS>
+cudaError_t launch_recip_combine(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms,
+                                 cudaStream_t st) {
+    if (B->d32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(B->d32, ca, w);
+    pa::k_combine<NS><<<unsigned((ca.n_act + 255) / 256), 256, 0, st>>>(B->d32, ca, w);
+    return cudaGetLastError();
+}
+
 #define PA_DISPATCH_NS(N, EXPR)                              \
     switch (N) {                                             \
         case 1: { constexpr int NSV = 1; EXPR; } break;      \
@@ -833,7 +844,19 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     PA_CUDA(ctx, ctx->fine_start.ensure(sizeof(int32_t) * (nfine + 1)));
     PA_CUDA(ctx, ctx->bin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
     PA_CUDA(ctx, ctx->tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
-    PA_CUDA(ctx, ctx->counters.ensure(sizeof(int32_t) * 8));
+    PA_CUDA(ctx, ctx->counters.ensure(sizeof(int32_t) * 16));  // [0, 8) insertions, [8, 16) items
+    if (f32) {
+        const int64_t nit = n_act * N;
+        PA_CUDA(ctx, ctx->item_bin.ensure(sizeof(int32_t) * nit));
+        PA_CUDA(ctx, ctx->item_slot.ensure(sizeof(int32_t) * nit));
+        PA_CUDA(ctx, ctx->item_sorted.ensure(sizeof(int32_t) * nit));
+        PA_CUDA(ctx, ctx->dUs.ensure(sizeof(double) * nit));
+        PA_CUDA(ctx, ctx->dUr.ensure(sizeof(double) * n_act));
+        PA_CUDA(ctx, ctx->item_count.ensure(sizeof(int32_t) * (nfine + 1)));
+        PA_CUDA(ctx, ctx->item_fine_start.ensure(sizeof(int32_t) * (nfine + 1)));
+        PA_CUDA(ctx, ctx->item_bin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+        PA_CUDA(ctx, ctx->item_tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+    }
     PA_CUDA(ctx, ctx->seg_out.ensure(sizeof(double) * 3 * nseg));
     // per-call tables, uploaded only when they differ from the last call's
     PA_CUDA(ctx, upload_cached(ctx->seg_rng, ctx->up_seg_rng, seg_rng, st));
@@ -861,7 +884,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_seg), sizeof(double) * 3 * nseg));
         ctx->h_seg_cap = size_t(3 * nseg);
     }
-    if (!ctx->h_cnt) PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_cnt), sizeof(int32_t) * 8));
+    if (!ctx->h_cnt) PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_cnt), sizeof(int32_t) * 16));
     pa::Work w{};
     if (f32) { w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>(); }
     else { w.pose64a = ctx->pose_a.as<double4>(); w.pose64b = ctx->pose_b.as<double4>(); }
@@ -869,6 +892,16 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     w.dU = ctx->dU.as<double>(); w.bin_count = ctx->bin_count.as<int32_t>(); w.fine_start = ctx->fine_start.as<int32_t>(); w.bin_start = ctx->bin_start.as<int32_t>();
     w.tile_start = ctx->tile_start.as<int32_t>(); w.counters = ctx->counters.as<int32_t>();
     w.seg_out = ctx->seg_out.as<double>(); w.seg_rng = ctx->seg_rng.as<int64_t>();
+    pa::Work wi = w;  // the item-level view: its own sort arrays and counters
+    if (f32) {
+        w.item_bin = ctx->item_bin.as<int32_t>(); w.item_slot = ctx->item_slot.as<int32_t>();
+        w.item_count = ctx->item_count.as<int32_t>(); w.dUs = ctx->dUs.as<double>(); w.dUr = ctx->dUr.as<double>();
+        wi = w;
+        wi.bin_of = w.item_bin; wi.slot = w.item_slot; wi.sorted = ctx->item_sorted.as<int32_t>();
+        wi.bin_count = w.item_count; wi.fine_start = ctx->item_fine_start.as<int32_t>();
+        wi.bin_start = ctx->item_bin_start.as<int32_t>(); wi.tile_start = ctx->item_tile_start.as<int32_t>();
+        wi.counters = ctx->counters.as<int32_t>() + 8;
+    }
     pa::CallArgs ca{};
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
@@ -883,7 +916,8 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     // sums, and the copies of the segment sums and counters into pinned host memory
     auto enqueue = [&]() -> pa_status {
         PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
-        PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 8, st));
+        PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 16, st));
+        if (f32) PA_CUDA(ctx, cudaMemsetAsync(ctx->item_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
         {
             Timer tm(ctx, 0);
             if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, ctx->rho2.as<float>(), ctx->reach0.as<int32_t>(), st))); }
@@ -895,15 +929,28 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             Timer tm(ctx, 1);
             pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
             pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
-            tm.stop(2);
+            int nl = 2;
+            if (f32) {
+                pa::k_scan<<<1, 1024, 0, st>>>(wi, B->nbins, nsub, PA_TILE32);
+                pa::k_scatter<<<unsigned((n_act * N + 255) / 256), 256, 0, st>>>(wi, n_act * N);
+                nl += 2;
+            }
+            tm.stop(nl);
             PA_CUDA(ctx, cudaGetLastError());
         }
         {
             Timer tm(ctx, 2);
             cudaError_t e = cudaSuccess;
-            PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, ctas, st)));
+            PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, f32 ? wi : w, ctx->num_sms, ctas, st)));
             tm.stop(1);
             if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+        }
+        if (f32) {
+            Timer tm(ctx, 6);
+            cudaError_t e = cudaSuccess;
+            PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B, ca, w, ctx->num_sms, st)));
+            tm.stop(B->d32.has_charge ? 2 : 1);
+            if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("reciprocal kernel launch: ") + cudaGetErrorString(e));
         }
         {
             Timer tm(ctx, 3);
@@ -912,7 +959,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             PA_CUDA(ctx, cudaGetLastError());
         }
         PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_seg, ctx->seg_out.p, sizeof(double) * 3 * nseg, cudaMemcpyDeviceToHost, st));
-        PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_cnt, ctx->counters.p, sizeof(int32_t) * 8, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_cnt, ctx->counters.p, sizeof(int32_t) * 16, cudaMemcpyDeviceToHost, st));
         return PA_OK;
     };
     if (ctx->tuning.use_graphs && !ctx->timing) {
@@ -920,15 +967,17 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         // arguments (the batch's device view byte for byte, so a re-upload of the same batch into
         // the same pooled addresses replays) and the workspace addresses
         struct GraphKey {
-            const void* ptrs[19];
+            const void* ptrs[28];
             int64_t i_lo, n_act, nseg, nfine;
             int32_t nbins, N, f32, reject, ctas, pad;
         } key;
         std::memset(&key, 0, sizeof(key));
-        const void* ps[19] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
+        const void* ps[28] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
                               ctx->bin_count.p, ctx->fine_start.p, ctx->bin_start.p, ctx->tile_start.p, ctx->counters.p,
                               ctx->seg_out.p, ctx->seg_rng.p, ctx->sys_off.p, ctx->rho2.p, ctx->reach0.p, ctx->scal.p,
-                              ctx->h_seg};
+                              ctx->h_seg, ctx->h_cnt, ctx->item_bin.p, ctx->item_slot.p, ctx->item_sorted.p,
+                              ctx->item_count.p, ctx->item_fine_start.p, ctx->item_bin_start.p, ctx->item_tile_start.p,
+                              ctx->dUs.p};
         std::memcpy(key.ptrs, ps, sizeof(ps));
         key.i_lo = i_lo; key.n_act = n_act; key.nseg = nseg; key.nfine = nfine;
         key.nbins = B->nbins; key.N = N; key.f32 = f32 ? 1 : 0; key.reject = ca.reject; key.ctas = ctas;
@@ -974,7 +1023,8 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     pa_status ws = wait_stream(ctx);
     if (ws != PA_OK) return ws;
     if (ctx->timing) Timer::collect(ctx);
-    if (counters[2] != 0) return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
+    if (counters[2] != 0 || counters[10] != 0)
+        return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
     if (per && per->flags)
         for (int64_t t = 0; t < n_act; ++t) per->flags[i_lo + t] = bin_of[t] < 0 ? 1 : 0;
     if (per && per->poses)
@@ -1197,6 +1247,7 @@ pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, con
 namespace {
 
 constexpr int64_t ST_MAX_INSERT = 131072;         // insertions per call
+constexpr int64_t ST_MAX_ITEMS = 3 * ST_MAX_INSERT;  // (insertion, guest site) items of the FP32 path
 constexpr int64_t ST_MAX_BINS = 32768;            // spatial bins of the batch
 constexpr int64_t ST_MAX_FINE = ST_MAX_BINS * 8;  // sub-bins
 constexpr int64_t ST_MAX_SEG = 2048;              // PA_SEGMENT-insertion segments per call
@@ -1210,7 +1261,7 @@ constexpr size_t ST_REACH0 = st_up(ST_SEG_RNG + 16 * ST_MAX_SEG);
 constexpr size_t ST_RHO2 = st_up(ST_REACH0 + 12 * ST_MAX_SYS);
 constexpr size_t ST_INPUT_END = st_up(ST_RHO2 + 8 * ST_MAX_RHO2);
 constexpr size_t ST_COUNTERS = ST_INPUT_END;
-constexpr size_t ST_BIN_COUNT = st_up(ST_COUNTERS + 4 * 8);
+constexpr size_t ST_BIN_COUNT = st_up(ST_COUNTERS + 4 * 16);
 constexpr size_t ST_FINE_START = st_up(ST_BIN_COUNT + 4 * (ST_MAX_FINE + 1));
 constexpr size_t ST_BIN_START = st_up(ST_FINE_START + 4 * (ST_MAX_FINE + 1));
 constexpr size_t ST_TILE_START = st_up(ST_BIN_START + 4 * (ST_MAX_BINS + 1));
@@ -1221,11 +1272,20 @@ constexpr size_t ST_BIN_OF = st_up(ST_POSE_B + 32 * ST_MAX_INSERT);
 constexpr size_t ST_SLOT = st_up(ST_BIN_OF + 4 * ST_MAX_INSERT);
 constexpr size_t ST_SORTED = st_up(ST_SLOT + 4 * ST_MAX_INSERT);
 constexpr size_t ST_DU = st_up(ST_SORTED + 4 * ST_MAX_INSERT);
-constexpr size_t ST_END = st_up(ST_DU + 8 * ST_MAX_INSERT);
+constexpr size_t ST_DUR = st_up(ST_DU + 8 * ST_MAX_INSERT);
+constexpr size_t ST_ITEM_BIN = st_up(ST_DUR + 8 * ST_MAX_INSERT);
+constexpr size_t ST_ITEM_SLOT = st_up(ST_ITEM_BIN + 4 * ST_MAX_ITEMS);
+constexpr size_t ST_ITEM_SORTED = st_up(ST_ITEM_SLOT + 4 * ST_MAX_ITEMS);
+constexpr size_t ST_DUS = st_up(ST_ITEM_SORTED + 4 * ST_MAX_ITEMS);
+constexpr size_t ST_ITEM_COUNT = st_up(ST_DUS + 8 * ST_MAX_ITEMS);
+constexpr size_t ST_ITEM_FINE_START = st_up(ST_ITEM_COUNT + 4 * (ST_MAX_FINE + 1));
+constexpr size_t ST_ITEM_BIN_START = st_up(ST_ITEM_FINE_START + 4 * (ST_MAX_FINE + 1));
+constexpr size_t ST_ITEM_TILE_START = st_up(ST_ITEM_BIN_START + 4 * (ST_MAX_BINS + 1));
+constexpr size_t ST_END = st_up(ST_ITEM_TILE_START + 4 * (ST_MAX_BINS + 1));
 
 }  // namespace
 
-#define PA_STATIC_SCRATCH_BYTES (16u << 20)
+#define PA_STATIC_SCRATCH_BYTES (32u << 20)
 static_assert(ST_END <= PA_STATIC_SCRATCH_BYTES, "static scratch layout exceeds the array");
 
 static __device__ __align__(256) unsigned char pa_static_scratch[PA_STATIC_SCRATCH_BYTES];
@@ -1238,7 +1298,7 @@ unsigned char st_stage[ST_INPUT_END];  // host staging of the small per-call inp
 int64_t st_ns[ST_MAX_SYS];
 Seg st_segs[ST_MAX_SEG];
 double st_segout[3 * ST_MAX_SEG];
-int32_t st_counters[8];
+int32_t st_counters[16];
 
 }  // namespace
 
@@ -1259,6 +1319,10 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     if (ninsert > ST_MAX_INSERT)
         return fail(ctx, PA_ERR_ARG, "pa_widom_static: ninsert=" + std::to_string(ninsert) + " exceeds its maximum of " +
                                          std::to_string(ST_MAX_INSERT) + " insertions per call");
+    if (f32 && ninsert * N > ST_MAX_ITEMS)
+        return fail(ctx, PA_ERR_ARG, "pa_widom_static: ninsert=" + std::to_string(ninsert) + " times " + std::to_string(N) +
+                                         " guest sites exceeds its maximum of " + std::to_string(ST_MAX_ITEMS) +
+                                         " (insertion, site) items per call");
     if (nsys > ST_MAX_SYS || int64_t(B->nbins) > ST_MAX_BINS || int64_t(nsys) * N * nt > ST_MAX_RHO2)
         return fail(ctx, PA_ERR_ARG, "pa_widom_static: batch exceeds the static scratch limits (" +
                                          std::to_string(ST_MAX_SYS) + " systems, " + std::to_string(ST_MAX_BINS) +
@@ -1321,7 +1385,8 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     PA_CUDA(ctx, cudaMemcpyAsync(base, st_stage, ST_INPUT_END, cudaMemcpyHostToDevice, st));
     const int64_t nfine = int64_t(B->nbins) * nsub;
     PA_CUDA(ctx, cudaMemsetAsync(base + ST_BIN_COUNT, 0, sizeof(int32_t) * (nfine + 1), st));
-    PA_CUDA(ctx, cudaMemsetAsync(base + ST_COUNTERS, 0, sizeof(int32_t) * 8, st));
+    PA_CUDA(ctx, cudaMemsetAsync(base + ST_COUNTERS, 0, sizeof(int32_t) * 16, st));
+    if (f32) PA_CUDA(ctx, cudaMemsetAsync(base + ST_ITEM_COUNT, 0, sizeof(int32_t) * (nfine + 1), st));
     pa::Work w{};
     if (f32) { w.pose_a = reinterpret_cast<float4*>(base + ST_POSE_A); w.pose_b = reinterpret_cast<float4*>(base + ST_POSE_B); }
     else { w.pose64a = reinterpret_cast<double4*>(base + ST_POSE_A); w.pose64b = reinterpret_cast<double4*>(base + ST_POSE_B); }
@@ -1331,6 +1396,18 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     w.bin_start = reinterpret_cast<int32_t*>(base + ST_BIN_START); w.tile_start = reinterpret_cast<int32_t*>(base + ST_TILE_START);
     w.counters = reinterpret_cast<int32_t*>(base + ST_COUNTERS); w.seg_out = reinterpret_cast<double*>(base + ST_SEG_OUT);
     w.seg_rng = reinterpret_cast<const int64_t*>(base + ST_SEG_RNG);
+    pa::Work wi = w;
+    if (f32) {
+        w.item_bin = reinterpret_cast<int32_t*>(base + ST_ITEM_BIN); w.item_slot = reinterpret_cast<int32_t*>(base + ST_ITEM_SLOT);
+        w.item_count = reinterpret_cast<int32_t*>(base + ST_ITEM_COUNT);
+        w.dUs = reinterpret_cast<double*>(base + ST_DUS); w.dUr = reinterpret_cast<double*>(base + ST_DUR);
+        wi = w;
+        wi.bin_of = w.item_bin; wi.slot = w.item_slot; wi.sorted = reinterpret_cast<int32_t*>(base + ST_ITEM_SORTED);
+        wi.bin_count = w.item_count; wi.fine_start = reinterpret_cast<int32_t*>(base + ST_ITEM_FINE_START);
+        wi.bin_start = reinterpret_cast<int32_t*>(base + ST_ITEM_BIN_START);
+        wi.tile_start = reinterpret_cast<int32_t*>(base + ST_ITEM_TILE_START);
+        wi.counters = reinterpret_cast<int32_t*>(base + ST_COUNTERS) + 8;
+    }
     pa::CallArgs ca{};
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = reinterpret_cast<const int64_t*>(base + ST_SYS_OFF);
     ca.seed = args->seed; ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
@@ -1340,11 +1417,16 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     PA_CUDA(ctx, cudaGetLastError());
     pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
     pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
+    if (f32) {
+        pa::k_scan<<<1, 1024, 0, st>>>(wi, B->nbins, nsub, PA_TILE32);
+        pa::k_scatter<<<unsigned((n_act * N + 255) / 256), 256, 0, st>>>(wi, n_act * N);
+    }
     PA_CUDA(ctx, cudaGetLastError());
     {
         cudaError_t e = cudaSuccess;
         PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
-        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
+        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
+        if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B, ca, w, ctx->num_sms, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
     }
     pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT, nullptr);
@@ -1355,7 +1437,8 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
         PA_CUDA(ctx, cudaMemcpyAsync(per->dU + i_lo, base + ST_DU, sizeof(double) * n_act, cudaMemcpyDeviceToHost, st));
     pa_status ws = wait_stream(ctx);
     if (ws != PA_OK) return ws;
-    if (st_counters[2] != 0) return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
+    if (st_counters[2] != 0 || st_counters[10] != 0)
+        return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
     if (sums->segments)
         for (int64_t q = 0; q < nseg; ++q)
             for (int r = 0; r < 3; ++r) sums->segments[3 * (sb + q) + r] = st_segout[3 * q + r];

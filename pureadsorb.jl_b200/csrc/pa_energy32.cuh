@@ -1,13 +1,20 @@
-// k_energy32: the FP32 insertion-energy kernel (src/energy.jl:42-82 restated for spatial bins).
+// The FP32 insertion energy (src/energy.jl:42-82 restated for spatial bins), in two kernels.
 //
-// Persistent CTAs of PA_WARPS32 independent warps. A work item is one warp's tile: up to 32
-// survivors of one spatial bin, ordered by sub-bin so the 32 insertions are close together.
-// The warp streams its bin's imaged neighbour list (positions relative to the bin centre,
-// charge, type) through its own two shared-memory stages with cp.async.bulk copies completing
-// on its own mbarriers, so warps never wait for one another. One insertion per lane: FP32
-// Lennard-Jones + screened Coulomb pair terms inside the cutoffs with a compensated sum, then
-// the reciprocal cross term against per-bin FP64 phase factors with cos/sin recurrences along
-// k-vector rows. Included by pa_kernels.cuh after its helpers.
+// k_energy32: the real-space pair sum. A work item is one (surviving insertion, guest site);
+// items are binned and sorted by the position of their own site, so the 32 lanes of a warp tile
+// are 32 sites lying within a small region of one spatial bin (with whole insertions per lane,
+// the sites of a tile would spread over the bin plus the guest's extent, and the cutoff sphere of
+// some lane would cut through nearly every staged list entry). Persistent CTAs of PA_WARPS32
+// independent warps; each warp streams its bin's imaged neighbour list (positions relative to the
+// bin centre, charge, type) through its own two shared-memory stages with cp.async.bulk copies
+// completing on its own mbarriers, so warps never wait for one another. FP32 Lennard-Jones +
+// screened Coulomb inside the cutoffs with a compensated sum per item.
+//
+// k_recip32: the reciprocal cross term per insertion, over tiles of 32 insertions of one bin:
+// per-bin FP64 phase factors, then cos/sin recurrences along k-vector rows per lane.
+//
+// k_combine (pa_kernels.cuh) adds the site sums, the reciprocal term and the constant offset in a
+// fixed order. Included by pa_kernels.cuh after its helpers.
 #pragma once
 
 #define PA_WARPS32 4
@@ -27,19 +34,50 @@ __device__ __forceinline__ float ex2_ftz(float x) {
     return r;
 }
 
+// Fetches the next tile of a persistent warp: its bin and the [lo, hi) range of sorted entries.
+__device__ __forceinline__ bool next_tile(const Work& w, int32_t nbins, int32_t lane, int32_t& bin, int32_t& lo,
+                                          int32_t& hi) {
+    const unsigned FULL = 0xffffffffu;
+    const int32_t total_tiles = w.counters[1];
+    int32_t t = 0;
+    if (lane == 0) {
+        t = atomicAdd(&w.counters[0], 1);
+        if (t < total_tiles) {
+            bin = find_bin(w.tile_start, nbins, t);
+            lo = w.bin_start[bin] + (t - w.tile_start[bin]) * PA_TILE32;
+            hi = min(lo + PA_TILE32, w.bin_start[bin + 1]);
+        }
+    }
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= total_tiles) return false;
+    bin = __shfl_sync(FULL, bin, 0); lo = __shfl_sync(FULL, lo, 0); hi = __shfl_sync(FULL, hi, 0);
+    return true;
+}
+
+// Centre of bin `bin` of framework fw in fractional coordinates.
+__device__ __forceinline__ void bin_centre(const DevBatch<float>& b, int32_t fw, int32_t bin, float& cx, float& cy,
+                                           float& cz) {
+    const int32_t* nb = b.bin_dims + 3 * fw;
+    const int32_t lb = bin - b.bin_base[fw];
+    const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
+    cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
+    cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
+    cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
+}
+
 // EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms.
 template <int NS, bool EQCUT>
 __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(128) int32_t s_type[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[PA_WARPS32][2];
-    __shared__ float2 s_B[PA_WARPS32][PA_KCHUNK32];
-    __shared__ float4 s_kc[PA_WARPS32][PA_KCHUNK32];
+    __shared__ float4 s_site[NS];    // body-frame site offsets, and the site charge times KE
     extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    const unsigned FULL = 0xffffffffu;
     const int nt = b.ntypes;
     for (int x = tid; x < NS * nt; x += blockDim.x) { s_lj[x] = b.sig2[x]; s_lj[NS * nt + x] = b.eps4[x]; }
+    if (tid < NS) s_site[tid] = make_float4(b.gsite[3 * tid], b.gsite[3 * tid + 1], b.gsite[3 * tid + 2],
+                                            float(KE * double(b.gq[tid])));
     if (lane == 0) { mbar_init(&s_bar[wp][0], 1); mbar_init(&s_bar[wp][1], 1); mbar_fence_init(); }
     __syncthreads();  // the only CTA-wide barrier: tables and barriers are ready
     const float* s_sig2 = s_lj;
@@ -48,28 +86,10 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     int32_t(*typ)[PA_CHUNK32] = s_type[wp];
     uint64_t* bar = s_bar[wp];
     uint32_t gchunk = 0;  // chunks this warp has consumed (selects stage and parity)
-    const int32_t total_tiles = w.counters[1];
-    float gqs[NS], gqk[NS], gsb[3 * NS];  // site charges, charges times the Coulomb constant, sites
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        gqs[s] = b.gq[s];
-        gqk[s] = float(KE * double(b.gq[s]));
-        gsb[3 * s] = b.gsite[3 * s]; gsb[3 * s + 1] = b.gsite[3 * s + 1]; gsb[3 * s + 2] = b.gsite[3 * s + 2];
-    }
     const bool charged = b.has_charge != 0;
-    for (;;) {
-        int32_t t = 0, bin = 0, lo = 0, hi = 0;
-        if (lane == 0) {
-            t = atomicAdd(&w.counters[0], 1);
-            if (t < total_tiles) {
-                bin = find_bin(w.tile_start, b.nbins, t);
-                lo = w.bin_start[bin] + (t - w.tile_start[bin]) * PA_TILE32;
-                hi = min(lo + PA_TILE32, w.bin_start[bin + 1]);
-            }
-        }
-        t = __shfl_sync(FULL, t, 0);
-        if (t >= total_tiles) break;
-        bin = __shfl_sync(FULL, bin, 0); lo = __shfl_sync(FULL, lo, 0); hi = __shfl_sync(FULL, hi, 0);
+    const unsigned FULL = 0xffffffffu;
+    int32_t bin = 0, lo = 0, hi = 0;
+    while (next_tile(w, b.nbins, lane, bin, lo, hi)) {
         const int32_t fw = b.bin_fw[bin];
         const int32_t l0 = b.list_offsets[bin], l1 = b.list_offsets[bin + 1];
         const int32_t nch = (l1 - l0 + PA_CHUNK32 - 1) / PA_CHUNK32;
@@ -84,45 +104,41 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             }
         }
         const bool active = lo + lane < hi;
-        const int32_t li = active ? w.sorted[lo + lane] : 0;
-        const int32_t* nb = b.bin_dims + 3 * fw;
-        const int32_t lb = bin - b.bin_base[fw];
-        const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
-        const float cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
-        const float cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
-        const float cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
+        const int32_t it = active ? w.sorted[lo + lane] : 0;
+        const int32_t li = it / NS, as = it - li * NS;  // insertion and site of this lane's item
+        float cx, cy, cz;
+        bin_centre(b, fw, bin, cx, cy, cz);
         const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
         const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
         const float* A = b.cells + 9 * fw;
         const float* iA = b.invcells + 9 * fw;
-        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
-        // site positions relative to the bin centre (Cartesian) and their fractional offsets
-        float px[NS], py[NS], pz[NS], dfr[3 * NS];
+        // the site relative to the bin centre: A (rp + shift - c) + g
+        float px, py, pz;
         {
             const float q[4] = {pq.x, pq.y, pq.z, pq.w};
-            const float c0 = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0));
-            const float c1 = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0));
-            const float c2 = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0));
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                float g[3];
-                rotate_s(q, gsb + 3 * s, g);
-                px[s] = c0 + g[0]; py[s] = c1 + g[1]; pz[s] = c2 + g[2];
-                dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
-                dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
-                dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
-            }
+            const float4 gs = s_site[as];
+            const float gb[3] = {gs.x, gs.y, gs.z};
+            float g[3], fs[3], sh[3];
+            rotate_s(q, gb, g);
+            const float rp[3] = {pa.x, pa.y, pa.z};
+            site_frac32(rp, g, iA, fs, sh);
+            // rp + shift - c is exact in FP64 (all three are FP32 values), then rounded once
+            const float d0 = float((double(pa.x) + double(sh[0])) - double(cx));
+            const float d1 = float((double(pa.y) + double(sh[1])) - double(cy));
+            const float d2 = float((double(pa.z) + double(sh[2])) - double(cz));
+            px = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0)) + g[0];
+            py = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0)) + g[1];
+            pz = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0)) + g[2];
         }
+        const float qk = s_site[as].w;
         const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
-        float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
-        // LJ parameters of the current type for each site: list entries come in runs of one type,
-        // and the type is the same for every lane, so the reload is a uniform branch
-        int32_t cur = -1;
-        float sg[NS], ep[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) { sg[s] = 0.f; ep[s] = 0.f; }
         const float NLOG2E = -1.4426950408889634f;
         const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
+        float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
+        // LJ parameters of the current host type for this lane's site: list entries come in runs of
+        // one type, the same for every lane, so the reload is a uniform branch
+        int32_t cur = -1;
+        float sg = 0.f, ep = 0.f;
         // tmo_at: chunk whose copy did not arrive in time (-1: none); after it no copies are issued
         // and only the chunk already in flight is still waited for
         int32_t tmo_at = -1;
@@ -133,51 +149,44 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             if (late && tmo_at < 0) tmo_at = c;
             const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
             if (tmo_at < 0) {
-#pragma unroll 2
+#pragma unroll 4
                 for (int32_t j = 0; j < n; ++j) {
                     const float4 at = xyzq[st][j];
                     const int32_t ty = typ[st][j];
                     if (ty != cur) {
                         cur = ty;
-#pragma unroll
-                        for (int s = 0; s < NS; ++s) { sg[s] = s_sig2[s * nt + ty]; ep[s] = s_eps4[s * nt + ty]; }
+                        sg = s_sig2[as * nt + ty];
+                        ep = s_eps4[as * nt + ty];
                     }
-                    // the entry's site terms are summed plainly (at most NS of them), and that sum
-                    // enters the compensated per-insertion sum once per entry
-                    float ee = 0.f;
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        if (r2 < rc2) {
-                            float e = 0.f;
-                            if (charged) {
-                                // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
-                                float ri = rsqrt_ftz(r2);
-                                ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
-                                if (EQCUT || r2 < rl2) {
-                                    const float x = sg[s] * (ri * ri);
-                                    const float x3 = x * x * x;
-                                    e = ep[s] * (x3 * x3 - x3);
-                                }
-                                if (EQCUT || r2 < re2) {
-                                    const float z = alpha * (r2 * ri);
-                                    const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
-                                    const float cf[PA_NERFC32] = PA_ERFC32_INIT;
-                                    float p = cf[PA_NERFC32 - 1];
-#pragma unroll
-                                    for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
-                                    e = fmaf(gqk[s] * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
-                                }
-                            } else {
-                                const float x = sg[s] * rcp_nr(r2);
+                    const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
+                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    if (r2 < rc2) {
+                        float e = 0.f;
+                        if (charged) {
+                            // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
+                            float ri = rsqrt_ftz(r2);
+                            ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
+                            if (EQCUT || r2 < rl2) {
+                                const float x = sg * (ri * ri);
                                 const float x3 = x * x * x;
-                                e = ep[s] * (x3 * x3 - x3);
+                                e = ep * (x3 * x3 - x3);
                             }
-                            ee += e;
+                            if (EQCUT || r2 < re2) {
+                                const float z = alpha * (r2 * ri);
+                                const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
+                                const float cf[PA_NERFC32] = PA_ERFC32_INIT;
+                                float p = cf[PA_NERFC32 - 1];
+#pragma unroll
+                                for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
+                                e = fmaf(qk * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
+                            }
+                        } else {
+                            const float x = sg * rcp_nr(r2);
+                            const float x3 = x * x * x;
+                            e = ep * (x3 * x3 - x3);
                         }
+                        kahan_add(esum, ecmp, e);
                     }
-                    kahan_add(esum, ecmp, ee);
                 }
             }
             __syncwarp();  // the warp is done with stage st
@@ -194,63 +203,97 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             if (lane == 0) atomicExch(&w.counters[2], 1);
             return;
         }
-        // Reciprocal term: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c} built in
-        // FP64 per bin, G_k = Σ_s q_s e^{2 pi i n.d_s} with d_s the site's fractional offset from
-        // the bin centre. Along a row of equal (n1, n2), n3 advances by the framework's step, so
-        // e^{2 pi i n.d_s} is carried by one complex multiplication and evaluated directly only
-        // at row starts.
-        double elr = 0.0;
-        if (charged) {
-            const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
-            float stc[NS], sts[NS], cr[NS], ci[NS];
-            const float kst = b.kstep[fw];
+        if (active) w.dUs[it] = double(esum) - double(ecmp);
+    }
+}
+
+// Reciprocal term per insertion: E_lr = Σ_k Re(B_k G_k), B_k = 2 kpref conj(S_k) e^{2 pi i n.c}
+// built in FP64 per bin, G_k = Σ_s q_s e^{2 pi i n.d_s} with d_s the site's fractional offset from
+// the bin centre. Along a row of equal (n1, n2), n3 advances by the framework's step, so
+// e^{2 pi i n.d_s} is carried by one complex multiplication and evaluated directly only at row
+// starts. Tiles of 32 insertions of one bin (insertion order, not site order); writes KE E_lr.
+template <int NS>
+__global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, CallArgs ca, Work w) {
+    __shared__ float2 s_B[PA_WARPS32][PA_KCHUNK32];
+    __shared__ float4 s_kc[PA_WARPS32][PA_KCHUNK32];
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    float gqs[NS], gsb[3 * NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        gqs[s] = b.gq[s];
+        gsb[3 * s] = b.gsite[3 * s]; gsb[3 * s + 1] = b.gsite[3 * s + 1]; gsb[3 * s + 2] = b.gsite[3 * s + 2];
+    }
+    int32_t bin = 0, lo = 0, hi = 0;
+    while (next_tile(w, b.nbins, lane, bin, lo, hi)) {
+        const int32_t fw = b.bin_fw[bin];
+        const bool active = lo + lane < hi;
+        const int32_t li = active ? w.sorted[lo + lane] : 0;
+        float cx, cy, cz;
+        bin_centre(b, fw, bin, cx, cy, cz);
+        const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
+        const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
+        const float* iA = b.invcells + 9 * fw;
+        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
+        float dfr[3 * NS];
+        {
+            const float q[4] = {pq.x, pq.y, pq.z, pq.w};
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
-                sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
-                cr[s] = 1.f; ci[s] = 0.f;
+                float g[3];
+                rotate_s(q, gsb + 3 * s, g);
+                dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
+                dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
+                dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
             }
-            float acc = 0.f, cacc = 0.f;
-            for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
-                const int32_t kn = min(PA_KCHUNK32, k1 - kb);
-                for (int32_t x = lane; x < kn; x += 32) {
-                    const int32_t kk = kb + x;
-                    const float4 kc = b.kcoef4[kk];
-                    s_kc[wp][x] = kc;
-                    double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
-                    ph -= rint(ph);
-                    double sn, cs;
-                    sincospi(2.0 * ph, &sn, &cs);
-                    const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
-                    // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
-                    s_B[wp][x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
-                }
-                __syncwarp();
-                for (int32_t x = 0; x < kn; ++x) {
-                    const float4 kc = s_kc[wp][x];
-                    if (kc.w == 0.f) {  // row start: direct evaluation
-#pragma unroll
-                        for (int s = 0; s < NS; ++s) {
-                            const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
-                            sincospif(2.0f * ph, &ci[s], &cr[s]);
-                        }
-                    } else {  // next k-vector of the row
-#pragma unroll
-                        for (int s = 0; s < NS; ++s) {
-                            const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
-                            ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
-                            cr[s] = r;
-                        }
-                    }
-                    float gr = 0.f, gi = 0.f;
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
-                    const float2 B = s_B[wp][x];
-                    kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
-                }
-                __syncwarp();
-            }
-            elr = double(acc) - double(cacc);
         }
-        if (active) w.dU[li] = double(esum) - double(ecmp) + KE * elr + b.const_offset[fw];
+        const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
+        float stc[NS], sts[NS], cr[NS], ci[NS];
+        const float kst = b.kstep[fw];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
+            cr[s] = 1.f; ci[s] = 0.f;
+        }
+        float acc = 0.f, cacc = 0.f;
+        for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
+            const int32_t kn = min(PA_KCHUNK32, k1 - kb);
+            for (int32_t x = lane; x < kn; x += 32) {
+                const int32_t kk = kb + x;
+                const float4 kc = b.kcoef4[kk];
+                s_kc[wp][x] = kc;
+                double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
+                ph -= rint(ph);
+                double sn, cs;
+                sincospi(2.0 * ph, &sn, &cs);
+                const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
+                // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
+                s_B[wp][x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
+            }
+            __syncwarp();
+            for (int32_t x = 0; x < kn; ++x) {
+                const float4 kc = s_kc[wp][x];
+                if (kc.w == 0.f) {  // row start: direct evaluation
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
+                        sincospif(2.0f * ph, &ci[s], &cr[s]);
+                    }
+                } else {  // next k-vector of the row
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
+                        ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
+                        cr[s] = r;
+                    }
+                }
+                float gr = 0.f, gi = 0.f;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
+                const float2 B = s_B[wp][x];
+                kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
+            }
+            __syncwarp();
+        }
+        if (active) w.dUr[li] = KE * (double(acc) - double(cacc));
     }
 }

@@ -94,6 +94,13 @@ struct Work {
     int32_t* counters;    // [0] tile cursor, [1] total tiles, [2] error code, [3] survivors
     double* seg_out;      // 3 per segment: max, Σ w, Σ ΔU w
     const int64_t* seg_rng;  // 2 per segment: local [begin, end)
+    // FP32 path: one work item per (survivor, guest site), binned by the site's own position
+    // (NULL item_bin: the FP64 path, whose items are the insertions themselves)
+    int32_t* item_bin;    // n_act*NS: sub-bin of the item's site, -1 if the insertion was rejected
+    int32_t* item_slot;   // n_act*NS
+    int32_t* item_count;  // nbins*nsub+1: items per sub-bin
+    double* dUs;          // n_act*NS: real-space energy of each item's site
+    double* dUr;          // n_act: KE times the reciprocal cross term
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -185,6 +192,37 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
     return false;
 }
 
+// Fractional position of a guest site: rp + A^-1 g (g the rotated body-frame offset), wrapped into
+// [0, 1); wrap gets the lattice shift -floor(rp + A^-1 g). k_pose bins each site with it and
+// k_energy32 places the site against its bin with the same shift, so both see the same image.
+__device__ __forceinline__ void site_frac32(const float rp[3], const float g[3], const float* iA, float fs[3],
+                                            float wrap[3]) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float f = rp[r] + fmaf(iA[6 + r], g[2], fmaf(iA[3 + r], g[1], iA[r] * g[0]));
+        wrap[r] = -floorf(f);
+        float w = f + wrap[r];
+        if (!(w < 1.0f)) {  // f just below an integer rounds up: it is the next image's 0
+            w = 0.0f;
+            wrap[r] -= 1.0f;
+        }
+        fs[r] = w;
+    }
+}
+
+// Sub-bin (bin * nsub + octant) of a fractional position in [0, 1) of framework fw.
+template <typename F>
+__device__ __forceinline__ int32_t sub_bin_of(const DevBatch<F>& b, int32_t fw, float x, float y, float z) {
+    const int32_t* nb = b.bin_dims + 3 * fw;
+    const float fx = x * float(nb[0]), fy = y * float(nb[1]), fz = z * float(nb[2]);
+    const int32_t bx = min(int32_t(fx), nb[0] - 1), by = min(int32_t(fy), nb[1] - 1), bz = min(int32_t(fz), nb[2] - 1);
+    const int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
+    int32_t sub = 0;
+    if (b.nsub == 8)
+        sub = int32_t(fx - float(bx) >= 0.5f) | (int32_t(fy - float(by) >= 0.5f) << 1) | (int32_t(fz - float(bz) >= 0.5f) << 2);
+    return bin * b.nsub + sub;
+}
+
 // ---------------------------------------------------------------------------------------------
 // k_pose: pose, phase 0, bin slot
 // ---------------------------------------------------------------------------------------------
@@ -208,6 +246,8 @@ __global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w
     if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0)) {
         w.bin_of[t] = -1;
         w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+        if (w.item_bin)
+            for (int a = 0; a < NS; ++a) w.item_bin[t * NS + a] = -1;
         return;
     }
     // spatial bin of the pose's reference point; with nsub = 8 the octant inside it orders the
@@ -222,6 +262,40 @@ __global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w
     const int32_t fine = bin * b.nsub + sub;
     w.bin_of[t] = fine;
     w.slot[t] = atomicAdd(&w.bin_count[fine], 1);
+    if constexpr (sizeof(F) == 4) {
+        if (w.item_bin) {  // each site into the sub-bin of its own position
+            const float* iAf = b.invcells + 9 * fw;
+            const float q[4] = {float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3])};
+            const float rpf[3] = {float(rp[0]), float(rp[1]), float(rp[2])};
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                const float gb[3] = {b.gsite[3 * a], b.gsite[3 * a + 1], b.gsite[3 * a + 2]};
+                float g[3], fs[3], sh[3];
+                rotate_s(q, gb, g);
+                site_frac32(rpf, g, iAf, fs, sh);
+                const int32_t sf = sub_bin_of(b, fw, fs[0], fs[1], fs[2]);
+                w.item_bin[t * NS + a] = sf;
+                w.item_slot[t * NS + a] = atomicAdd(&w.item_count[sf], 1);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_combine (FP32 path): ΔU = Σ_sites (real-space site sums) + KE E_lr + constant offset, in a
+// fixed order; rejected insertions keep +inf.
+// ---------------------------------------------------------------------------------------------
+template <int NS>
+__global__ void __launch_bounds__(256) k_combine(DevBatch<float> b, CallArgs ca, Work w) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= ca.n_act || w.bin_of[t] < 0) return;
+    const int32_t s = find_system(ca.sys_off, b.nsys, ca.i_lo + t);
+    const int32_t fw = b.framework_of[s];
+    double e = w.dUs[t * NS];
+#pragma unroll
+    for (int a = 1; a < NS; ++a) e += w.dUs[t * NS + a];
+    if (b.has_charge) e += w.dUr[t];
+    w.dU[t] = e + b.const_offset[fw];
 }
 
 // ---------------------------------------------------------------------------------------------

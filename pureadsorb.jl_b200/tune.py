@@ -33,15 +33,15 @@ def _device_ms(ctx, call, repeats):
         call()
         ms, n = ctx.kernel_times()
         ctx.set_timing(False)
-        times.append(float(np.sum(ms[:4])))
+        times.append(float(np.sum(ms[:4]) + ms[6]))
     return float(np.median(times))
 
 
 def autotune(batch, guest, *, T, ninsert, backend=None, seed=0, nblocks=10, run=None, bin_widths=BIN_WIDTHS,
              ctas_per_sm=CTAS_PER_SM, repeats=2):
     """Times widom(batch, guest; T, ninsert, seed, nblocks, run) on the device for every
-    (bin width, CTAs per SM) candidate (device time of the pose, scan, energy and reduction
-    kernels, median of `repeats` calls after one warm-up) and sets the fastest on the backend's
+    (bin width, CTAs per SM) candidate (device time of the pose, scan, energy, reciprocal and
+    reduction kernels, median of `repeats` calls after one warm-up) and sets the fastest on the backend's
     context; the batch is re-uploaded with the chosen bin width. Returns a TuneReport."""
     backend = backend or default_backend()
     ctx = backend.ctx
