@@ -373,11 +373,6 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     std::vector<int32_t> bdims(3 * nfw), bbase(nfw + 1, 0), bfw;
     std::vector<double> radius2(nfw);
     std::vector<int32_t> nimg(nfw);
-    double rg = 0;
-    for (int a = 0; a < N; ++a)
-        rg = std::max(rg, std::sqrt(desc->guest_sites[3 * a] * desc->guest_sites[3 * a] +
-                                    desc->guest_sites[3 * a + 1] * desc->guest_sites[3 * a + 1] +
-                                    desc->guest_sites[3 * a + 2] * desc->guest_sites[3 * a + 2]));
     const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
     double binw = ctx->tuning.bin_width > 0 ? ctx->tuning.bin_width : DEFAULT_BIN_WIDTH;
     for (int fw = 0; fw < nfw; ++fw) {
@@ -397,7 +392,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
                 for (int r = 0; r < 3; ++r) v[r] = A[r] * d[0] + A[r + 3] * d[1] + A[r + 6] * d[2];
                 circ = std::max(circ, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
             }
-        double R = rcmax + rg + circ + 1.0e-3;
+        // every FP32 work item is one guest site, binned by the site's own position: its pairs
+        // lie within rc of a point of its bin
+        double R = rcmax + circ + 1.0e-3;
         radius2[fw] = R * R;
         // an image n of a fractional offset d in [-1/2, 1/2]^3 lies within R only if
         // |d_r + n_r| <= R / L_r on every axis, so |n_r| <= floor(R / L_r + 1/2)
@@ -1109,7 +1106,7 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
     PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.as<int32_t>() + 4, 0, sizeof(int32_t), st));
     pa::Work w{};
     w.pose_a = ctx->pose_a.as<float4>(); w.pose_b = ctx->pose_b.as<float4>();
-    w.bin_of = ctx->bin_of.as<int32_t>(); w.dU = ctx->dU.as<double>();
+    w.bin_of = ctx->bin_of.as<int32_t>(); w.dU = ctx->dU.as<double>(); w.item_bin = ctx->item_bin.as<int32_t>();
     pa::CallArgs ca{};
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;

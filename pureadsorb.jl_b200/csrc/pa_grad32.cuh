@@ -50,13 +50,13 @@ __global__ void __launch_bounds__(256) k_heavy(Work w, CallArgs ca, GradArgs g) 
     if (keep) g.heavy[base + __popc(bal & ((1u << lane) - 1u))] = int32_t(t);
 }
 
-// One warp per recomputed insertion; the lanes stride over the insertion's bin list (then over
-// the framework's k-vectors). The site geometry is the forward kernel's, operation for operation.
+// One warp per recomputed insertion. For each guest site the lanes stride over the list of the
+// bin holding that site (the forward pass's (insertion, site) items), with the forward kernel's
+// site geometry operation for operation; then over the framework's k-vectors.
 template <int NS>
 __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, CallArgs ca, Work w, GradArgs g) {
     extern __shared__ float s_dyn[];  // sig2 (NS*nt), then per warp 2*NS*nt accumulators
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    const unsigned FULL = 0xffffffffu;
     const int nt = b.ntypes, nacc = 2 * NS * nt;
     float* s_sig2 = s_dyn;
     float* acc = s_dyn + NS * nt + wp * nacc;
@@ -72,73 +72,63 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
     const bool charged = b.has_charge != 0;
     const int32_t nh = *g.nheavy;
     const int32_t nwarps = gridDim.x * PA_WARPSG;
+    const float NLOG2E = -1.4426950408889634f;
     for (int32_t h = blockIdx.x * PA_WARPSG + wp; h < nh; h += nwarps) {
         const int32_t li = g.heavy[h];
-        const int32_t bin = w.bin_of[li] / b.nsub;  // bin_of holds the sub-bin bin * nsub + octant
         const int32_t sy = find_system(ca.sys_off, g.nsys, ca.i_lo + li);
         const double wgt = exp(-w.dU[li] / g.kT - g.xmax[sy]);
-        const int32_t fw = b.bin_fw[bin];
-        const int32_t l0 = b.list_offsets[bin], l1 = b.list_offsets[bin + 1];
-        const int32_t* nb = b.bin_dims + 3 * fw;
-        const int32_t lb = bin - b.bin_base[fw];
-        const int32_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / (nb[0] * nb[1]);
-        const float cx = __fdiv_rn(float(bx) + 0.5f, float(nb[0]));
-        const float cy = __fdiv_rn(float(by) + 0.5f, float(nb[1]));
-        const float cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
+        const double wke = wgt * KE;
         const float4 pa = w.pose_a[li];
         const float4 pq = w.pose_b[li];
+        const float q[4] = {pq.x, pq.y, pq.z, pq.w};
+        const float rp[3] = {pa.x, pa.y, pa.z};
+        const int32_t fw = b.framework_of[sy];
         const float* A = b.cells + 9 * fw;
         const float* iA = b.invcells + 9 * fw;
-        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
-        float px[NS], py[NS], pz[NS], dfr[3 * NS];
-        {
-            const float q[4] = {pq.x, pq.y, pq.z, pq.w};
-            const float c0 = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0));
-            const float c1 = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0));
-            const float c2 = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0));
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                float gg[3];
-                rotate_s(q, gsb + 3 * s, gg);
-                px[s] = c0 + gg[0]; py[s] = c1 + gg[1]; pz[s] = c2 + gg[2];
-                dfr[3 * s + 0] = d0 + fmaf(iA[6], gg[2], fmaf(iA[3], gg[1], iA[0] * gg[0]));
-                dfr[3 * s + 1] = d1 + fmaf(iA[7], gg[2], fmaf(iA[4], gg[1], iA[1] * gg[0]));
-                dfr[3 * s + 2] = d2 + fmaf(iA[8], gg[2], fmaf(iA[5], gg[1], iA[2] * gg[0]));
-            }
-        }
         const float rl2 = b.rl2, re2 = b.re2, alpha = float(b.alphas[fw]);
-        const float NLOG2E = -1.4426950408889634f;
-        const double wke = wgt * KE;
         double* gq_sys = g.g_q + g.sys_aoff[sy] - b.atom_offsets[fw];
-        // per-lane sums for the lane's current host type, flushed to the warp's shared
-        // accumulators when the type changes (the list is type-major, so changes are rare)
-        int32_t cur = -1;
-        float P[NS], Q[NS];
+        double fr[3 * NS];  // absolute fractional site positions (reciprocal phases)
 #pragma unroll
-        for (int s = 0; s < NS; ++s) { P[s] = 0.f; Q[s] = 0.f; }
-        for (int32_t e = l0 + lane; e < l1; e += 32) {
-            const float4 at = b.list_xyzq[e];
-            const int32_t ty = b.list_type[e];
-            if (ty != cur) {
-                if (cur >= 0)
+        for (int s = 0; s < NS; ++s) {
+            float gg[3], fs[3], sh[3];
+            rotate_s(q, gsb + 3 * s, gg);
+            site_frac32(rp, gg, iA, fs, sh);
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        if (P[s] != 0.f) atomicAdd(&acc[s * nt + cur], P[s]);
-                        if (Q[s] != 0.f) atomicAdd(&acc[(NS + s) * nt + cur], Q[s]);
-                        P[s] = 0.f; Q[s] = 0.f;
+            for (int r = 0; r < 3; ++r)
+                fr[3 * s + r] = double(rp[r]) + double(fmaf(iA[6 + r], gg[2], fmaf(iA[3 + r], gg[1], iA[r] * gg[0])));
+            // this site's bin and its position relative to the bin centre (as in k_energy32)
+            const int32_t bin = w.item_bin[li * NS + s] / b.nsub;
+            const int32_t l0 = b.list_offsets[bin], l1 = b.list_offsets[bin + 1];
+            float cx, cy, cz;
+            bin_centre(b, fw, bin, cx, cy, cz);
+            const float d0 = float((double(pa.x) + double(sh[0])) - double(cx));
+            const float d1 = float((double(pa.y) + double(sh[1])) - double(cy));
+            const float d2 = float((double(pa.z) + double(sh[2])) - double(cz));
+            const float px = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0)) + gg[0];
+            const float py = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0)) + gg[1];
+            const float pz = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0)) + gg[2];
+            // per-lane sums for the lane's current host type, flushed to the warp's shared
+            // accumulators when the type changes (the list is type-major, so changes are rare)
+            int32_t cur = -1;
+            float P = 0.f, Q = 0.f;
+            for (int32_t e = l0 + lane; e < l1; e += 32) {
+                const float4 at = b.list_xyzq[e];
+                const int32_t ty = b.list_type[e];
+                if (ty != cur) {
+                    if (cur >= 0) {
+                        if (P != 0.f) atomicAdd(&acc[s * nt + cur], P);
+                        if (Q != 0.f) atomicAdd(&acc[(NS + s) * nt + cur], Q);
+                        P = 0.f; Q = 0.f;
                     }
-                cur = ty;
-            }
-            float cq = 0.f;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                const float dx = px[s] - at.x, dy = py[s] - at.y, dz = pz[s] - at.z;
+                    cur = ty;
+                }
+                const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
                 const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 if (r2 < rl2) {
                     const float x = s_sig2[s * nt + ty] * rcp_nr(r2);
                     const float x3 = x * x * x;
-                    P[s] = fmaf(x3, x3 - 1.0f, P[s]);
-                    Q[s] = fmaf(x3, fmaf(2.0f, x3, -1.0f), Q[s]);
+                    P = fmaf(x3, x3 - 1.0f, P);
+                    Q = fmaf(x3, fmaf(2.0f, x3, -1.0f), Q);
                 }
                 if (charged && r2 < re2) {
                     float ri = rsqrt_ftz(r2);
@@ -149,17 +139,15 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
                     float p = cf[PA_NERFC32 - 1];
 #pragma unroll
                     for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
-                    cq = fmaf(gqs[s], p * ex2_ftz((z * z) * NLOG2E) * ri, cq);
+                    const float cq = gqs[s] * (p * ex2_ftz((z * z) * NLOG2E) * ri);
+                    if (cq != 0.f) atomicAdd(&gq_sys[b.list_atom[e]], wke * double(cq));
                 }
             }
-            if (cq != 0.f) atomicAdd(&gq_sys[b.list_atom[e]], wke * double(cq));
-        }
-        if (cur >= 0)
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                if (P[s] != 0.f) atomicAdd(&acc[s * nt + cur], P[s]);
-                if (Q[s] != 0.f) atomicAdd(&acc[(NS + s) * nt + cur], Q[s]);
+            if (cur >= 0) {
+                if (P != 0.f) atomicAdd(&acc[s * nt + cur], P);
+                if (Q != 0.f) atomicAdd(&acc[(NS + s) * nt + cur], Q);
             }
+        }
         __syncwarp();
         double* glj = g.g_lj + int64_t(sy) * nacc;
         for (int x = lane; x < nacc; x += 32) {
@@ -167,17 +155,10 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
             if (v != 0.f) { atomicAdd(&glj[x], wgt * double(v)); acc[x] = 0.f; }
         }
         __syncwarp();
-        // G_k += w S_g(k): the phase n.(c + d_a) of every site in FP64, one k-vector per lane
+        // G_k += w S_g(k): the phase n.r_a of every site in FP64, one k-vector per lane
         if (charged) {
             const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
             double* gk = g.g_k + 2 * (g.sys_koff[sy] - k0);
-            double fr[3 * NS];
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                fr[3 * s] = double(cx) + double(dfr[3 * s]);
-                fr[3 * s + 1] = double(cy) + double(dfr[3 * s + 1]);
-                fr[3 * s + 2] = double(cz) + double(dfr[3 * s + 2]);
-            }
             for (int32_t kk = k0 + lane; kk < k1; kk += 32) {
                 const float4 kc = b.kcoef4[kk];
                 double gr = 0.0, gi = 0.0;
