@@ -28,7 +28,7 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
 # DRAM bytes (read + write) of one k_energy32 launch on this workload, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
-ENERGY32_TRAFFIC_BYTES = 101.298688e6 + 4.943616e6
+ENERGY32_TRAFFIC_BYTES = 96.518656e6 + 8.461312e6
 
 
 def parse():
