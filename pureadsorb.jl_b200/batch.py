@@ -238,6 +238,8 @@ class FrameworkBatch:
         self._offset_parts = offset_parts
         self.bs = self._hardcore_bounds()
         self._device = {}
+        self._desc = None      # desc() result; a FrameworkBatch is not modified after construction
+        self._rejection = {}   # rejection tables per (kT, eps)
 
     def _hardcore_bounds(self):
         """B_s per framework (src/batch.jl:409-423)."""
@@ -271,6 +273,8 @@ class FrameworkBatch:
         new.constant_offset = np.array([tail_delta(ff, counts, self._gcounts, V) + ke + sm
                                         for ke, sm, counts, V in self._offset_parts])
         new._device = {}
+        new._desc = None
+        new._rejection = {}
         if move_device:
             for key, dev in self._device.items():
                 dev.set_pair_tables(new.sigma, new.epsilon, new.constant_offset)
@@ -310,7 +314,12 @@ class FrameworkBatch:
                                         f"must equal its atom count {nat}")
 
     def desc(self):
-        """(pa_batch_desc, arrays it points into): the C-ABI view of this batch."""
+        """(pa_batch_desc, arrays it points into): the C-ABI view of this batch, built once."""
+        if getattr(self, "_desc", None) is None:
+            self._desc = self._make_desc()
+        return self._desc
+
+    def _make_desc(self):
         col = lambda M: np.ascontiguousarray(np.transpose(M, (0, 2, 1)).reshape(-1))  # column-major per matrix
         arr = {
             "positions": np.ascontiguousarray(self.positions.reshape(-1), dtype=np.float64),

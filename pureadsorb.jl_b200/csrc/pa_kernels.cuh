@@ -227,7 +227,7 @@ __device__ __forceinline__ int32_t sub_bin_of(const DevBatch<F>& b, int32_t fw, 
 // k_pose: pose, phase 0, bin slot
 // ---------------------------------------------------------------------------------------------
 template <typename F, int NS>
-__global__ void __launch_bounds__(256) k_pose(DevBatch<F> b, CallArgs ca, Work w, const F* rho2, const int32_t* reach0) {
+__global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Work w, const F* rho2, const int32_t* reach0) {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= ca.n_act) return;
     const int64_t i = ca.i_lo + t;

@@ -62,7 +62,11 @@ def build_rejection_tables(batch, kT):
     """Rejection radii rho2 (nsys*N*ntypes) and phase-0 stencil half-widths reach0 (nsys x 3) for
     one call (src/widom.jl:202-253), computed by the library's host code (pa_rejection_tables).
     The summation-error term uses eps of the batch's float type; theta is theta_F(Float64)
-    because weights accumulate in FP64."""
+    because weights accumulate in FP64. Cached on the batch per (kT, eps)."""
+    key = (float(kT), float(np.finfo(batch.T).eps))
+    cache = getattr(batch, "_rejection", None)
+    if cache is not None and key in cache:
+        return cache[key]
     N = len(batch.guest_types)
     nt = len(batch.sigma)
     d, keep = batch.desc()
@@ -78,6 +82,10 @@ def build_rejection_tables(batch, kT):
         s = bad.value
         raise ArgumentError(f"build_rejection_tables: system {s} has no valid rejection radius (margin <= 0 or a "
                             f"root search failed; kT={kT}, theta_F={float(theta_F(np.float64))})")
+    rho2.flags.writeable = False
+    reach0.flags.writeable = False
+    if cache is not None:
+        cache[key] = (rho2, reach0)
     return rho2, reach0
 
 
