@@ -58,6 +58,8 @@ struct pa_context {
         sys_off, rho2, reach0;
     // FP32 path: (insertion, site) work items
     DevMem item_bin, item_slot, item_sorted, item_count, item_fine_start, item_bin_start, item_tile_start, dUs, dUr;
+    // FP32 path: every insertion in sub-bin order, for phase 0
+    DevMem abin, aslot, asorted, acount, afine_start, abin_start, atile_start;
     // adjoint workspace
     DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
     // launch choices, the replayable graph of the last call's device sequence and its key
@@ -853,6 +855,13 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         PA_CUDA(ctx, ctx->item_fine_start.ensure(sizeof(int32_t) * (nfine + 1)));
         PA_CUDA(ctx, ctx->item_bin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
         PA_CUDA(ctx, ctx->item_tile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+        PA_CUDA(ctx, ctx->abin.ensure(sizeof(int32_t) * n_act));
+        PA_CUDA(ctx, ctx->aslot.ensure(sizeof(int32_t) * n_act));
+        PA_CUDA(ctx, ctx->asorted.ensure(sizeof(int32_t) * n_act));
+        PA_CUDA(ctx, ctx->acount.ensure(sizeof(int32_t) * (nfine + 1)));
+        PA_CUDA(ctx, ctx->afine_start.ensure(sizeof(int32_t) * (nfine + 1)));
+        PA_CUDA(ctx, ctx->abin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+        PA_CUDA(ctx, ctx->atile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
     }
     PA_CUDA(ctx, ctx->seg_out.ensure(sizeof(double) * 3 * nseg));
     // per-call tables, uploaded only when they differ from the last call's
@@ -899,6 +908,13 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         wi.bin_start = ctx->item_bin_start.as<int32_t>(); wi.tile_start = ctx->item_tile_start.as<int32_t>();
         wi.counters = ctx->counters.as<int32_t>() + 8;
     }
+    pa::Work wa = w;  // the all-insertion view (FP32 phase 0 in sub-bin order)
+    if (f32) {
+        wa.bin_of = ctx->abin.as<int32_t>(); wa.slot = ctx->aslot.as<int32_t>(); wa.sorted = ctx->asorted.as<int32_t>();
+        wa.bin_count = ctx->acount.as<int32_t>(); wa.fine_start = ctx->afine_start.as<int32_t>();
+        wa.bin_start = ctx->abin_start.as<int32_t>(); wa.tile_start = ctx->atile_start.as<int32_t>();
+        wa.counters = ctx->counters.as<int32_t>() + 12;
+    }
     pa::CallArgs ca{};
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
@@ -914,11 +930,33 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     auto enqueue = [&]() -> pa_status {
         PA_CUDA(ctx, cudaMemsetAsync(ctx->bin_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
         PA_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, sizeof(int32_t) * 16, st));
-        if (f32) PA_CUDA(ctx, cudaMemsetAsync(ctx->item_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
-        {
+        if (f32) {
+            PA_CUDA(ctx, cudaMemsetAsync(ctx->item_count.p, 0, sizeof(int32_t) * (nfine + 1), st));
+            PA_CUDA(ctx, cudaMemsetAsync(ctx->acount.p, 0, sizeof(int32_t) * (nfine + 1), st));
+        }
+        if (f32) {
+            const unsigned gr = unsigned((n_act + 255) / 256);
+            {
+                Timer tm(ctx, 0);
+                PA_DISPATCH_NS(N, (pa::k_draw32<NSV><<<gr, 256, 0, st>>>(B->d32, ca, w, wa)));
+                tm.stop(1);
+            }
+            {
+                Timer tm(ctx, 1);
+                pa::k_scan<<<1, 1024, 0, st>>>(wa, B->nbins, nsub, PA_TILE32);
+                pa::k_scatter<<<gr, 256, 0, st>>>(wa, n_act);
+                tm.stop(2);
+            }
+            {
+                Timer tm(ctx, 0);
+                PA_DISPATCH_NS(N, (pa::k_phase0_32<NSV><<<gr, 256, 0, st>>>(B->d32, ca, w, wa.sorted, ctx->rho2.as<float>(),
+                                                                               ctx->reach0.as<int32_t>())));
+                tm.stop(1);
+            }
+            PA_CUDA(ctx, cudaGetLastError());
+        } else {
             Timer tm(ctx, 0);
-            if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, ctx->rho2.as<float>(), ctx->reach0.as<int32_t>(), st))); }
-            else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, ctx->rho2.as<double>(), ctx->reach0.as<int32_t>(), st))); }
+            PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, ctx->rho2.as<double>(), ctx->reach0.as<int32_t>(), st)));
             tm.stop(1);
             PA_CUDA(ctx, cudaGetLastError());
         }
@@ -964,17 +1002,18 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         // arguments (the batch's device view byte for byte, so a re-upload of the same batch into
         // the same pooled addresses replays) and the workspace addresses
         struct GraphKey {
-            const void* ptrs[28];
+            const void* ptrs[36];
             int64_t i_lo, n_act, nseg, nfine;
             int32_t nbins, N, f32, reject, ctas, pad;
         } key;
         std::memset(&key, 0, sizeof(key));
-        const void* ps[28] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
+        const void* ps[36] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
                               ctx->bin_count.p, ctx->fine_start.p, ctx->bin_start.p, ctx->tile_start.p, ctx->counters.p,
                               ctx->seg_out.p, ctx->seg_rng.p, ctx->sys_off.p, ctx->rho2.p, ctx->reach0.p, ctx->scal.p,
                               ctx->h_seg, ctx->h_cnt, ctx->item_bin.p, ctx->item_slot.p, ctx->item_sorted.p,
                               ctx->item_count.p, ctx->item_fine_start.p, ctx->item_bin_start.p, ctx->item_tile_start.p,
-                              ctx->dUs.p};
+                              ctx->dUs.p, ctx->abin.p, ctx->aslot.p, ctx->asorted.p, ctx->acount.p, ctx->afine_start.p,
+                              ctx->abin_start.p, ctx->atile_start.p, ctx->dUr.p};
         std::memcpy(key.ptrs, ps, sizeof(ps));
         key.i_lo = i_lo; key.n_act = n_act; key.nseg = nseg; key.nfine = nfine;
         key.nbins = B->nbins; key.N = N; key.f32 = f32 ? 1 : 0; key.reject = ca.reject; key.ctas = ctas;

@@ -224,42 +224,23 @@ __device__ __forceinline__ int32_t sub_bin_of(const DevBatch<F>& b, int32_t fw, 
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_pose: pose, phase 0, bin slot
+// Outcome of phase 0 for insertion t: a rejected insertion gets bin -1 and ΔU = +inf; a survivor
+// a slot in its centre's sub-bin and, on the FP32 path, one (insertion, site) item per guest site
+// in the sub-bin of the site's own position.
 // ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mark_rejected(const Work& w, int64_t t, int ns) {
+    w.bin_of[t] = -1;
+    w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    if (w.item_bin)
+        for (int a = 0; a < ns; ++a) w.item_bin[t * ns + a] = -1;
+}
+
 template <typename F, int NS>
-__global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Work w, const F* rho2, const int32_t* reach0) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= ca.n_act) return;
-    const int64_t i = ca.i_lo + t;
-    const int32_t s = find_system(ca.sys_off, b.nsys, i);
-    const int64_t k = i - ca.sys_off[s] + 1;
-    const int32_t fw = b.framework_of[s];
-    F rp[3], qt[4];
-    draw_pose<F>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
-    if (sizeof(F) == 4) {
-        w.pose_a[t] = make_float4(float(rp[0]), float(rp[1]), float(rp[2]), 0.0f);
-        w.pose_b[t] = make_float4(float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3]));
-    } else {
-        w.pose64a[t] = make_double4(double(rp[0]), double(rp[1]), double(rp[2]), 0.0);
-        w.pose64b[t] = make_double4(double(qt[0]), double(qt[1]), double(qt[2]), double(qt[3]));
-    }
-    if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0)) {
-        w.bin_of[t] = -1;
-        w.dU[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
-        if (w.item_bin)
-            for (int a = 0; a < NS; ++a) w.item_bin[t * NS + a] = -1;
-        return;
-    }
+__device__ __forceinline__ void bin_survivor(const DevBatch<F>& b, const Work& w, int64_t t, int32_t fw, const F* rp,
+                                             const F* qt) {
     // spatial bin of the pose's reference point; with nsub = 8 the octant inside it orders the
     // survivors, so that a warp's 32 insertions lie in two adjacent octants
-    const int32_t* nb = b.bin_dims + 3 * fw;
-    const float fx = float(rp[0]) * float(nb[0]), fy = float(rp[1]) * float(nb[1]), fz = float(rp[2]) * float(nb[2]);
-    const int32_t bx = min(int32_t(fx), nb[0] - 1), by = min(int32_t(fy), nb[1] - 1), bz = min(int32_t(fz), nb[2] - 1);
-    const int32_t bin = b.bin_base[fw] + bx + nb[0] * (by + nb[1] * bz);
-    int32_t sub = 0;
-    if (b.nsub == 8)
-        sub = int32_t(fx - float(bx) >= 0.5f) | (int32_t(fy - float(by) >= 0.5f) << 1) | (int32_t(fz - float(bz) >= 0.5f) << 2);
-    const int32_t fine = bin * b.nsub + sub;
+    const int32_t fine = sub_bin_of(b, fw, float(rp[0]), float(rp[1]), float(rp[2]));
     w.bin_of[t] = fine;
     w.slot[t] = atomicAdd(&w.bin_count[fine], 1);
     if constexpr (sizeof(F) == 4) {
@@ -279,6 +260,74 @@ __global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Wor
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_pose: pose, phase 0, bin slot (one thread per insertion, in insertion order)
+// ---------------------------------------------------------------------------------------------
+template <typename F, int NS>
+__global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Work w, const F* rho2, const int32_t* reach0) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= ca.n_act) return;
+    const int64_t i = ca.i_lo + t;
+    const int32_t s = find_system(ca.sys_off, b.nsys, i);
+    const int64_t k = i - ca.sys_off[s] + 1;
+    const int32_t fw = b.framework_of[s];
+    F rp[3], qt[4];
+    draw_pose<F>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    if (sizeof(F) == 4) {
+        w.pose_a[t] = make_float4(float(rp[0]), float(rp[1]), float(rp[2]), 0.0f);
+        w.pose_b[t] = make_float4(float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3]));
+    } else {
+        w.pose64a[t] = make_double4(double(rp[0]), double(rp[1]), double(rp[2]), 0.0);
+        w.pose64b[t] = make_double4(double(qt[0]), double(qt[1]), double(qt[2]), double(qt[3]));
+    }
+    if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0)) {
+        mark_rejected(w, t, NS);
+        return;
+    }
+    bin_survivor<F, NS>(b, w, t, fw, rp, qt);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The FP32 path splits k_pose in two so that phase 0 runs in spatial order: k_draw32 draws every
+// pose and gives it a slot in its centre's sub-bin (a scan and scatter then order all insertions
+// by sub-bin), and k_phase0_32 scans the hard core of the insertions in that order. Neighbouring
+// threads then walk nearly the same cells and mostly reach the same outcome, where insertion
+// order gives every thread an unrelated stencil and exit point.
+// ---------------------------------------------------------------------------------------------
+template <int NS>
+__global__ void __launch_bounds__(256) k_draw32(DevBatch<float> b, CallArgs ca, Work w, Work wa) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= ca.n_act) return;
+    const int64_t i = ca.i_lo + t;
+    const int32_t s = find_system(ca.sys_off, b.nsys, i);
+    const int64_t k = i - ca.sys_off[s] + 1;
+    const int32_t fw = b.framework_of[s];
+    float rp[3], qt[4];
+    draw_pose<float>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    w.pose_a[t] = make_float4(rp[0], rp[1], rp[2], 0.0f);
+    w.pose_b[t] = make_float4(qt[0], qt[1], qt[2], qt[3]);
+    const int32_t fine = sub_bin_of(b, fw, rp[0], rp[1], rp[2]);
+    wa.bin_of[t] = fine;
+    wa.slot[t] = atomicAdd(&wa.bin_count[fine], 1);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256, 4) k_phase0_32(DevBatch<float> b, CallArgs ca, Work w, const int32_t* order,
+                                                      const float* rho2, const int32_t* reach0) {
+    const int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= ca.n_act) return;
+    const int64_t t = order[x];
+    const int32_t s = find_system(ca.sys_off, b.nsys, ca.i_lo + t);
+    const int32_t fw = b.framework_of[s];
+    const float4 pa = w.pose_a[t], pq = w.pose_b[t];
+    const float rp[3] = {pa.x, pa.y, pa.z}, qt[4] = {pq.x, pq.y, pq.z, pq.w};
+    if (ca.reject && hardcore_scan<float, NS>(b, s, fw, rp, qt, rho2, reach0)) {
+        mark_rejected(w, t, NS);
+        return;
+    }
+    bin_survivor<float, NS>(b, w, t, fw, rp, qt);
 }
 
 // ---------------------------------------------------------------------------------------------
