@@ -108,6 +108,9 @@ class FrameworkBatch:
         kmax = ewald_kmax(alpha, ewald.precision)
         neutral = bool(np.all(guest.charges == 0))
         self_quats = self_term_quaternions() if not neutral else None
+        # the guest's site offsets at every self-term orientation (the same for every framework)
+        self_sites = (np.array([[_rotate(q, s) for s in guest.sites] for q in self_quats]) if not neutral
+                      else None)
 
         # compact LJ types: framework atoms' types union the guest's (src/batch.jl:309-317)
         ty_orig = [np.array([ff.typeindex(s + "_") for s in fw.symbols], dtype=np.int64) for fw in unique]
@@ -171,7 +174,7 @@ class FrameworkBatch:
                 kcoeffs.append(coeffs[sel])
                 samples = np.empty(SELF_TERM_NORIENT)
                 for o in range(SELF_TERM_NORIENT):
-                    gs = np.array([_rotate(self_quats[o], s) for s in guest.sites])
+                    gs = self_sites[o]
                     ph = kv_full @ gs.T
                     Sg = np.cos(ph) @ guest.charges + 1j * (np.sin(ph) @ guest.charges)
                     samples[o] = KE * float(np.sum(kpref_full * np.abs(Sg) ** 2))

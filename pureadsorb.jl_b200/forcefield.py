@@ -24,11 +24,17 @@ class ForceField:
         self.tail = bool(tail)
 
     def typeindex(self, name):
-        """1-based index of a type name (src/forcefield.jl:41-45)."""
-        try:
-            return self.names.index(name) + 1
-        except ValueError:
-            raise ArgumentError(f"unknown LJ type {name}; force field defines {self.names}") from None
+        """1-based index of a type name (src/forcefield.jl:41-45); the first of equal names."""
+        index = self.__dict__.get("_index")
+        if index is None:
+            index = {}
+            for i, n in enumerate(self.names):
+                index.setdefault(n, i + 1)
+            self._index = index
+        i = index.get(name)
+        if i is None:
+            raise ArgumentError(f"unknown LJ type {name}; force field defines {self.names}")
+        return i
 
 
 def read_forcefield(path, T=np.float64):
