@@ -480,7 +480,7 @@ def main():
                 "clocks": clk.summary(),
                 "tuning": {"bin_width": tune.bin_width, "ctas_per_sm": tune.ctas_per_sm, "cuda_graphs": True,
                            "candidates": [list(r) for r in tune.table]},
-                "gpu_launches": int(9 * args.steps),
+                "gpu_launches": int(10 * args.steps),
                 "kernel_ms": {"pose_phase0": kms[0] / args.steps, "scan_scatter": kms[1] / args.steps,
                               "energy": kms[2] / args.steps, "reciprocal_combine": kms[6] / args.steps,
                               "segment_reduce": kms[3] / args.steps},

@@ -943,8 +943,8 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             }
             {
                 Timer tm(ctx, 1);
-                pa::k_scan<<<1, 1024, 0, st>>>(wa, B->nbins, nsub, PA_TILE32);
-                pa::k_scatter<<<gr, 256, 0, st>>>(wa, n_act);
+                pa::k_scan<<<1, 1024, 0, st>>>(pa::sort_view(wa), B->nbins, nsub, PA_TILE32);
+                pa::k_scatter<<<gr, 256, 0, st>>>(pa::sort_view(wa), n_act);
                 tm.stop(2);
             }
             {
@@ -962,15 +962,14 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         }
         {
             Timer tm(ctx, 1);
-            pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
-            pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
-            int nl = 2;
-            if (f32) {
-                pa::k_scan<<<1, 1024, 0, st>>>(wi, B->nbins, nsub, PA_TILE32);
-                pa::k_scatter<<<unsigned((n_act * N + 255) / 256), 256, 0, st>>>(wi, n_act * N);
-                nl += 2;
+            if (f32) {  // the survivors' and the items' sorts side by side
+                pa::k_scan2<<<2, 1024, 0, st>>>(pa::sort_view(w), pa::sort_view(wi), B->nbins, nsub, PA_TILE32);
+                pa::k_scatter2<<<unsigned((n_act * (N + 1) + 255) / 256), 256, 0, st>>>(pa::sort_view(w), n_act, pa::sort_view(wi), n_act * N);
+            } else {
+                pa::k_scan<<<1, 1024, 0, st>>>(pa::sort_view(w), B->nbins, nsub, PA_TILE64);
+                pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(pa::sort_view(w), n_act);
             }
-            tm.stop(nl);
+            tm.stop(2);
             PA_CUDA(ctx, cudaGetLastError());
         }
         {
@@ -1451,11 +1450,11 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     if (f32) { PA_DISPATCH_NS(N, (launch_pose<float, NSV>(B, ca, w, reinterpret_cast<const float*>(base + ST_RHO2), reach0, st))); }
     else { PA_DISPATCH_NS(N, (launch_pose<double, NSV>(B, ca, w, reinterpret_cast<const double*>(base + ST_RHO2), reach0, st))); }
     PA_CUDA(ctx, cudaGetLastError());
-    pa::k_scan<<<1, 1024, 0, st>>>(w, B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
-    pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, n_act);
+    pa::k_scan<<<1, 1024, 0, st>>>(pa::sort_view(w), B->nbins, nsub, f32 ? PA_TILE32 : PA_TILE64);
+    pa::k_scatter<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(pa::sort_view(w), n_act);
     if (f32) {
-        pa::k_scan<<<1, 1024, 0, st>>>(wi, B->nbins, nsub, PA_TILE32);
-        pa::k_scatter<<<unsigned((n_act * N + 255) / 256), 256, 0, st>>>(wi, n_act * N);
+        pa::k_scan<<<1, 1024, 0, st>>>(pa::sort_view(wi), B->nbins, nsub, PA_TILE32);
+        pa::k_scatter<<<unsigned((n_act * N + 255) / 256), 256, 0, st>>>(pa::sort_view(wi), n_act * N);
     }
     PA_CUDA(ctx, cudaGetLastError());
     {

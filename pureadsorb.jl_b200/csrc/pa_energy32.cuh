@@ -254,7 +254,8 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
             sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
             cr[s] = 1.f; ci[s] = 0.f;
         }
-        float acc = 0.f, cacc = 0.f;
+        // the terms of one k-vector row (a few) are summed plainly, rows then compensated
+        float acc = 0.f, cacc = 0.f, row = 0.f;
         for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
             const int32_t kn = min(PA_KCHUNK32, k1 - kb);
             for (int32_t x = lane; x < kn; x += 32) {
@@ -272,7 +273,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
             __syncwarp();
             for (int32_t x = 0; x < kn; ++x) {
                 const float4 kc = s_kc[wp][x];
-                if (kc.w == 0.f) {  // row start: direct evaluation
+                if (kc.w == 0.f) {  // row start: direct evaluation; the finished row enters the sum
+                    kahan_add(acc, cacc, row);
+                    row = 0.f;
 #pragma unroll
                     for (int s = 0; s < NS; ++s) {
                         const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
@@ -290,10 +293,11 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
 #pragma unroll
                 for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
                 const float2 B = s_B[wp][x];
-                kahan_add(acc, cacc, fmaf(B.x, gr, -B.y * gi));
+                row = fmaf(B.x, gr, fmaf(-B.y, gi, row));
             }
             __syncwarp();
         }
+        kahan_add(acc, cacc, row);
         if (active) w.dUr[li] = KE * (double(acc) - double(cacc));
     }
 }

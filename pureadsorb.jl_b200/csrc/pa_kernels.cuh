@@ -376,13 +376,29 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* s_warp, i
     return warp_excl + x - v;
 }
 
-__global__ void __launch_bounds__(1024) k_scan(Work w, int32_t nbins, int32_t nsub, int32_t tile) {
+// The arrays of one sort, by value (a kernel parameter whose address is taken would be copied
+// to local memory).
+struct SortView {
+    const int32_t* count;
+    int32_t* fine_start;
+    int32_t* bin_start;
+    int32_t* tile_start;
+    int32_t* counters;
+    const int32_t* bin_of;
+    const int32_t* slot;
+    int32_t* sorted;
+};
+__host__ __device__ inline SortView sort_view(const Work& w) {
+    return SortView{w.bin_count, w.fine_start, w.bin_start, w.tile_start, w.counters, w.bin_of, w.slot, w.sorted};
+}
+
+__device__ __forceinline__ void scan_body(SortView w, int32_t nbins, int32_t nsub, int32_t tile) {
     __shared__ int32_t s_warp[32];
     const int32_t nfine = nbins * nsub;
     int32_t carry = 0;
     for (int32_t base = 0; base < nfine; base += blockDim.x) {  // survivors per sub-bin -> starts
         const int32_t f = base + threadIdx.x;
-        const int32_t c = f < nfine ? w.bin_count[f] : 0;
+        const int32_t c = f < nfine ? w.count[f] : 0;
         int32_t tot;
         const int32_t e = block_excl_scan(c, s_warp, &tot);
         if (f < nfine) w.fine_start[f] = carry + e;
@@ -412,11 +428,31 @@ __global__ void __launch_bounds__(1024) k_scan(Work w, int32_t nbins, int32_t ns
     }
 }
 
-__global__ void k_scatter(Work w, int64_t n_act) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= n_act) return;
-    int32_t bin = w.bin_of[t];
+__global__ void __launch_bounds__(1024) k_scan(SortView w, int32_t nbins, int32_t nsub, int32_t tile) {
+    scan_body(w, nbins, nsub, tile);
+}
+
+// Two independent scans in one launch, one CTA each (the survivors' and the items' sort).
+__global__ void __launch_bounds__(1024) k_scan2(SortView w0, SortView w1, int32_t nbins, int32_t nsub, int32_t tile) {
+    if (blockIdx.x == 0) scan_body(w0, nbins, nsub, tile);
+    else scan_body(w1, nbins, nsub, tile);
+}
+
+__device__ __forceinline__ void scatter_one(const SortView& w, int64_t t) {
+    const int32_t bin = w.bin_of[t];
     if (bin >= 0) w.sorted[w.fine_start[bin] + w.slot[t]] = int32_t(t);
+}
+
+__global__ void k_scatter(SortView w, int64_t n_act) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n_act) scatter_one(w, t);
+}
+
+// Two scatters in one launch: entries [0, n0) of w0, then [0, n1) of w1.
+__global__ void k_scatter2(SortView w0, int64_t n0, SortView w1, int64_t n1) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n0) scatter_one(w0, t);
+    else if (t - n0 < n1) scatter_one(w1, t - n0);
 }
 
 // ---------------------------------------------------------------------------------------------
