@@ -67,7 +67,9 @@ pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*7*/, int64_t* la
  * kernel, 1..8 (0 selects 8). use_graphs: 1 makes pa_widom capture its device sequence (kernels,
  * memsets and the copy of the segment sums into pinned host memory) in a CUDA graph and replay it
  * while the call's shape (batch, insertion range, workspace) repeats; seed and kT may change
- * between replays. Graphs are not used while per-kernel timing is on. */
+ * between replays. A shape is captured on its second consecutive call (the first runs directly),
+ * so a batch uploaded anew for every call never pays for a capture. Graphs are not used while
+ * per-kernel timing is on. */
 typedef struct pa_tuning {
     double bin_width;
     int32_t ctas_per_sm;

@@ -65,7 +65,7 @@ struct pa_context {
     // launch choices, the replayable graph of the last call's device sequence and its key
     pa_tuning tuning{0.0, 0, 0};
     cudaGraphExec_t gexec = nullptr;
-    std::vector<unsigned char> gkey;
+    std::vector<unsigned char> gkey, last_key;  // key of the captured graph, and of the last call
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
     // counters, and host copies of the last uploaded per-call tables (re-uploaded only on change)
     DevMem scal, bnd;
@@ -1020,21 +1020,30 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         std::vector<unsigned char> kb(kp, kp + sizeof(key));
         const unsigned char* vp = f32 ? reinterpret_cast<const unsigned char*>(&B->d32) : reinterpret_cast<const unsigned char*>(&B->d64);
         kb.insert(kb.end(), vp, vp + (f32 ? sizeof(B->d32) : sizeof(B->d64)));
-        if (!ctx->gexec || kb != ctx->gkey) {
-            if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
-            ctx->gkey.clear();
-            cudaGraph_t graph = nullptr;
-            PA_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const bool have = ctx->gexec && kb == ctx->gkey;
+        if (!have && kb != ctx->last_key) {
+            // a shape seen for the first time runs directly: capturing pays off from its
+            // second call on (a batch re-uploaded every call would otherwise capture every call)
+            ctx->last_key = kb;
             pa_status es = enqueue();
-            cudaError_t ee = cudaStreamEndCapture(st, &graph);
-            if (es != PA_OK) { if (graph) cudaGraphDestroy(graph); return es; }
-            PA_CUDA(ctx, ee);
-            cudaError_t ie = cudaGraphInstantiate(&ctx->gexec, graph, 0);
-            cudaGraphDestroy(graph);
-            if (ie != cudaSuccess) { ctx->gexec = nullptr; PA_CUDA(ctx, ie); }
-            ctx->gkey = kb;
+            if (es != PA_OK) return es;
+        } else {
+            if (!have) {
+                if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+                ctx->gkey.clear();
+                cudaGraph_t graph = nullptr;
+                PA_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                pa_status es = enqueue();
+                cudaError_t ee = cudaStreamEndCapture(st, &graph);
+                if (es != PA_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+                PA_CUDA(ctx, ee);
+                cudaError_t ie = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ie != cudaSuccess) { ctx->gexec = nullptr; PA_CUDA(ctx, ie); }
+                ctx->gkey = kb;
+            }
+            PA_CUDA(ctx, cudaGraphLaunch(ctx->gexec, st));
         }
-        PA_CUDA(ctx, cudaGraphLaunch(ctx->gexec, st));
     } else {
         pa_status es = enqueue();
         if (es != PA_OK) return es;

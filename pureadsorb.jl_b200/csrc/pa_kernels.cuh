@@ -708,7 +708,11 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
                          double(__fdiv_rn(float(by) + 0.5f, float(nb[1]))),
                          double(__fdiv_rn(float(bz) + 0.5f, float(nb[2])))};
     const double* A = g.cells + 9 * fw;
-    const double R2 = g.radius2[fw];
+    float Af[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) Af[r] = float(A[r]);
+    const float cf[3] = {float(c[0]), float(c[1]), float(c[2])};
+    const float R2f = float(g.radius2[fw]);
     const int32_t m = g.nimg[fw], side = 2 * m + 1, nimgs = side * side * side;
     const int32_t a0 = g.atom_offsets[fw], a1 = g.atom_offsets[fw + 1];
     const int64_t npairs = int64_t(a1 - a0) * nimgs;
@@ -718,23 +722,24 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     for (int64_t p0 = 0; p0 < npairs; p0 += blockDim.x) {
         const int64_t p = p0 + threadIdx.x;
         bool keep = false;
-        double dx = 0, dy = 0, dz = 0;
-        int32_t j = 0;
+        int32_t j = 0, n0 = 0, n1 = 0, n2 = 0;
         if (p < npairs) {
             j = g.order[a0 + int32_t(p / nimgs)];
             const int32_t im = int32_t(p % nimgs);
-            const int32_t n0 = im % side - m, n1 = (im / side) % side - m, n2 = im / (side * side) - m;
-            double d0 = St<double>::sub(g.frac[3 * j], c[0]), d1 = St<double>::sub(g.frac[3 * j + 1], c[1]),
-                   d2 = St<double>::sub(g.frac[3 * j + 2], c[2]);
-            // strict operations: the count and fill instantiations must keep identical sets
-            typedef St<double> S;
-            d0 = S::add(S::sub(d0, rint(d0)), double(n0));
-            d1 = S::add(S::sub(d1, rint(d1)), double(n1));
-            d2 = S::add(S::sub(d2, rint(d2)), double(n2));
-            dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
-            dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
-            dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
-            keep = dot3s(dx, dy, dz, dx, dy, dz) <= R2;
+            n0 = im % side - m; n1 = (im / side) % side - m; n2 = im / (side * side) - m;
+            // membership test in strict FP32: the count and fill instantiations keep identical sets,
+            // and R carries a margin far above FP32 rounding, so the list holds every image within
+            // the cutoff plus circumradius of the bin centre
+            typedef St<float> S;
+            float d0 = S::sub(float(g.frac[3 * j]), cf[0]), d1 = S::sub(float(g.frac[3 * j + 1]), cf[1]),
+                  d2 = S::sub(float(g.frac[3 * j + 2]), cf[2]);
+            d0 = S::add(S::sub(d0, rintf(d0)), float(n0));
+            d1 = S::add(S::sub(d1, rintf(d1)), float(n1));
+            d2 = S::add(S::sub(d2, rintf(d2)), float(n2));
+            const float x = dot3s(Af[0], Af[3], Af[6], d0, d1, d2);
+            const float y = dot3s(Af[1], Af[4], Af[7], d0, d1, d2);
+            const float z = dot3s(Af[2], Af[5], Af[8], d0, d1, d2);
+            keep = dot3s(x, y, z, x, y, z) <= R2f;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) s_warp[wid] = __popc(bal);
@@ -744,6 +749,16 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         if (FILL && keep) {
             const int32_t pos = s_base + before + __popc(bal & ((1u << lane) - 1u));
             if (pos < g.offsets[bin + 1]) {
+                // the stored position relative to the bin centre, in FP64 then rounded once
+                typedef St<double> S;
+                double d0 = S::sub(g.frac[3 * j], c[0]), d1 = S::sub(g.frac[3 * j + 1], c[1]),
+                       d2 = S::sub(g.frac[3 * j + 2], c[2]);
+                d0 = S::add(S::sub(d0, rint(d0)), double(n0));
+                d1 = S::add(S::sub(d1, rint(d1)), double(n1));
+                d2 = S::add(S::sub(d2, rint(d2)), double(n2));
+                const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
+                const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
+                const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
                 g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
                 g.type_out[pos] = g.types[j];
                 g.atom_out[pos] = j;

@@ -41,8 +41,10 @@ def autotune(batch, guest, *, T, ninsert, backend=None, seed=0, nblocks=10, run=
              ctas_per_sm=CTAS_PER_SM, repeats=2):
     """Times widom(batch, guest; T, ninsert, seed, nblocks, run) on the device for every
     (bin width, CTAs per SM) candidate (device time of the pose, scan, energy, reciprocal and
-    reduction kernels, median of `repeats` calls after one warm-up) and sets the fastest on the backend's
-    context; the batch is re-uploaded with the chosen bin width. Returns a TuneReport."""
+    reduction kernels, median of `repeats` calls after one warm-up) and sets the fastest on the
+    backend's context, preferring the widest bin among those within 2 % of the fastest (its
+    neighbour lists are the shortest to build and hold); the batch is re-uploaded with the chosen
+    bin width. Returns a TuneReport."""
     backend = backend or default_backend()
     ctx = backend.ctx
     old = ctx.tuning()
@@ -66,7 +68,8 @@ def autotune(batch, guest, *, T, ninsert, backend=None, seed=0, nblocks=10, run=
         ctx.set_tuning(bin_width=old.bin_width, ctas_per_sm=old.ctas_per_sm)
         batch.drop_device()
         raise
-    w, c, ms = min(table, key=lambda r: r[2])
+    best = min(r[2] for r in table)
+    w, c, ms = max((r for r in table if r[2] <= 1.02 * best), key=lambda r: (r[0], -r[2]))
     ctx.set_tuning(bin_width=w, ctas_per_sm=c)
     batch.drop_device()
     batch.device(ctx)
