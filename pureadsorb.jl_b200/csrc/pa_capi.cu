@@ -253,7 +253,10 @@ pa_status wait_stream(pa_context* ctx) {
         if (e != cudaErrorNotReady) return fail(ctx, PA_ERR_CUDA, std::string("device work failed: ") + cudaGetErrorString(e));
         double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (dt > WAIT_LIMIT_S) return fail(ctx, PA_ERR_TIMEOUT, "device work did not finish within the host wait limit");
-        std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.01 ? 20 : 500));
+        // poll without sleeping for the first 50 ms (a sleep of a few microseconds lasts tens of
+        // them), then back off
+        if (dt < 0.05) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(500));
     }
 }
 
