@@ -378,6 +378,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     std::vector<int32_t> bdims(3 * nfw), bbase(nfw + 1, 0), bfw;
     std::vector<double> radius2(nfw);
     std::vector<int32_t> nimg(nfw);
+    std::vector<float> reach(3 * nfw);
     const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
     double binw = ctx->tuning.bin_width > 0 ? ctx->tuning.bin_width : DEFAULT_BIN_WIDTH;
     for (int fw = 0; fw < nfw; ++fw) {
@@ -405,6 +406,8 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         // |d_r + n_r| <= R / L_r on every axis, so |n_r| <= floor(R / L_r + 1/2)
         double Lmin = std::min(L[0], std::min(L[1], L[2]));
         nimg[fw] = int32_t(std::floor(R / Lmin + 0.5));
+        // the per-axis image bound of the list build, widened far beyond FP32 rounding
+        for (int r = 0; r < 3; ++r) reach[3 * fw + r] = float(R / L[r] * (1.0 + 1.0e-6) + 1.0e-5);
     }
     B->nbins = bbase[nfw];
     // one packed upload of every table (and the list build's temporaries)
@@ -418,7 +421,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     const size_t t_q64 = pk.add(std::vector<double>(desc->charges, desc->charges + na));
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
     const bool lists = sizeof(F) == 4;
-    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0;
+    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0, t_reach = 0, t_fr32 = 0;
     if (lists) {
         std::vector<double> frac(3 * na), q(desc->charges, desc->charges + na);
         for (int fw = 0; fw < nfw; ++fw)
@@ -429,17 +432,26 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
                                       iA[r + 6] * desc->positions[3 * j + 2];
                 }
         std::vector<double> cells64(desc->cells, desc->cells + 9 * nfw);
-        // each framework's atoms in type-major order: list entries of one type form one run
-        std::vector<int32_t> order(na);
+        // each framework's atoms in type-major order (a stable counting sort): list entries of one
+        // type form one run; beside it the FP32 fractional coordinates in that order, which the
+        // list build's membership test reads coalesced
+        std::vector<int32_t> order(na), tstart(nt + 1);
+        std::vector<float4> fr32(na);
         for (int fw = 0; fw < nfw; ++fw) {
             const int32_t a0 = B->atom_offsets[fw], a1 = B->atom_offsets[fw + 1];
-            for (int32_t j = a0; j < a1; ++j) order[j] = j;
-            std::stable_sort(order.begin() + a0, order.begin() + a1,
-                             [&](int32_t x, int32_t y) { return types[x] < types[y]; });
+            std::fill(tstart.begin(), tstart.end(), 0);
+            for (int32_t j = a0; j < a1; ++j) ++tstart[types[j] + 1];
+            for (int t = 0; t < nt; ++t) tstart[t + 1] += tstart[t];
+            for (int32_t j = a0; j < a1; ++j) order[a0 + tstart[types[j]]++] = j;
+            for (int32_t rk = a0; rk < a1; ++rk) {
+                const int32_t j = order[rk];
+                fr32[rk] = make_float4(float(frac[3 * j]), float(frac[3 * j + 1]), float(frac[3 * j + 2]), 0.f);
+            }
         }
         t_order = pk.add(order);
+        t_fr32 = pk.add(fr32);
         t_frac = pk.add(frac); t_q = pk.add(q); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
-        t_nimg = pk.add(nimg); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
+        t_nimg = pk.add(nimg); t_reach = pk.add(reach); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
     }
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.host.size(), st));
     PA_CUDA(ctx, cudaMemcpyAsync(B->arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
@@ -455,10 +467,12 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         g.types = reinterpret_cast<const int32_t*>(base + o.types); g.cells = reinterpret_cast<const double*>(base + t_cells);
         g.atom_offsets = reinterpret_cast<const int32_t*>(base + o.atom_offsets);
         g.order = reinterpret_cast<const int32_t*>(base + t_order);
+        g.fr32 = reinterpret_cast<const float4*>(base + t_fr32);
         g.bin_dims = reinterpret_cast<const int32_t*>(base + o.bin_dims);
         g.bin_base = reinterpret_cast<const int32_t*>(base + o.bin_base);
         g.bin_fw = reinterpret_cast<const int32_t*>(base + o.bin_fw);
         g.radius2 = reinterpret_cast<const double*>(base + t_r2); g.nimg = reinterpret_cast<const int32_t*>(base + t_nimg);
+        g.reach = reinterpret_cast<const float*>(base + t_reach);
         g.counts = reinterpret_cast<int32_t*>(base + t_count);
         if (B->nbins > 0) {
             Timer tm(ctx, 4);
@@ -498,11 +512,11 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             tm.stop(1);
             PA_CUDA(ctx, cudaGetLastError());
         }
-        ws = wait_stream(ctx);
-        if (ws != PA_OK) return ws;
     }
     fill_batch_view(B, view<F>(B), desc, o);
-    return wait_stream(ctx);
+    // the fill pass is stream-ordered before every later use of the batch on this context, so the
+    // host does not wait for it (its errors surface at the next wait, like any kernel's)
+    return lists ? PA_OK : wait_stream(ctx);
 }
 
 template <typename F, int NS>

@@ -684,11 +684,13 @@ struct ListGeom {
     const double* cells;       // 9*nfw
     const int32_t* atom_offsets;
     const int32_t* order;      // natoms: the framework's atoms ordered by type (stable), global indices
+    const float4* fr32;        // natoms: FP32 fractional coordinates of order[rank], by rank
     const int32_t* bin_dims;   // 3*nfw
     const int32_t* bin_base;   // nfw+1
     const int32_t* bin_fw;     // nbins
     const double* radius2;     // nfw
     const int32_t* nimg;       // nfw: m
+    const float* reach;        // 3*nfw: R / L_r plus a margin (images beyond it are never kept)
     int32_t* counts;           // nbins (count pass)
     const int32_t* offsets;    // nbins+1 (fill pass)
     float4* xyzq;
@@ -696,6 +698,13 @@ struct ListGeom {
     int32_t* atom_out;         // stored-atom index of each entry (for the adjoint)
 };
 
+// Neighbour lists of the FP32 path: per bin, every atom image within R of the bin centre, in the
+// order (atom rank in `order`, image index) with the image index n0 + side (n1 + side n2) running
+// fastest. One thread per atom: an image can only lie within R if |d_r + n_r| <= R / L_r on each
+// axis (L_r the perpendicular width), so each thread tests only the images inside that box (a
+// margin far above FP32 rounding keeps every image the strict test would keep), then an ordered
+// block scan of the per-thread counts places its entries. Count and fill passes make the same
+// tests, so the fill writes exactly the counted entries.
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     __shared__ int32_t s_warp[8];
@@ -713,56 +722,79 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     for (int r = 0; r < 9; ++r) Af[r] = float(A[r]);
     const float cf[3] = {float(c[0]), float(c[1]), float(c[2])};
     const float R2f = float(g.radius2[fw]);
-    const int32_t m = g.nimg[fw], side = 2 * m + 1, nimgs = side * side * side;
+    const float reach[3] = {g.reach[3 * fw], g.reach[3 * fw + 1], g.reach[3 * fw + 2]};
+    const int32_t m = g.nimg[fw];
     const int32_t a0 = g.atom_offsets[fw], a1 = g.atom_offsets[fw + 1];
-    const int64_t npairs = int64_t(a1 - a0) * nimgs;
     if (threadIdx.x == 0) s_base = FILL ? g.offsets[bin] : 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int64_t p0 = 0; p0 < npairs; p0 += blockDim.x) {
-        const int64_t p = p0 + threadIdx.x;
-        bool keep = false;
-        int32_t j = 0, n0 = 0, n1 = 0, n2 = 0;
-        if (p < npairs) {
-            j = g.order[a0 + int32_t(p / nimgs)];
-            const int32_t im = int32_t(p % nimgs);
-            n0 = im % side - m; n1 = (im / side) % side - m; n2 = im / (side * side) - m;
-            // membership test in strict FP32: the count and fill instantiations keep identical sets,
-            // and R carries a margin far above FP32 rounding, so the list holds every image within
-            // the cutoff plus circumradius of the bin centre
-            typedef St<float> S;
-            float d0 = S::sub(float(g.frac[3 * j]), cf[0]), d1 = S::sub(float(g.frac[3 * j + 1]), cf[1]),
-                  d2 = S::sub(float(g.frac[3 * j + 2]), cf[2]);
-            d0 = S::add(S::sub(d0, rintf(d0)), float(n0));
-            d1 = S::add(S::sub(d1, rintf(d1)), float(n1));
-            d2 = S::add(S::sub(d2, rintf(d2)), float(n2));
-            const float x = dot3s(Af[0], Af[3], Af[6], d0, d1, d2);
-            const float y = dot3s(Af[1], Af[4], Af[7], d0, d1, d2);
-            const float z = dot3s(Af[2], Af[5], Af[8], d0, d1, d2);
-            keep = dot3s(x, y, z, x, y, z) <= R2f;
+    typedef St<float> S;
+    for (int32_t r0 = a0; r0 < a1; r0 += blockDim.x) {
+        const int32_t rk = r0 + int32_t(threadIdx.x);
+        int32_t j = 0, lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+        float d[3] = {0.f, 0.f, 0.f};
+        if (rk < a1) {
+            j = g.order[rk];
+            const float4 f = g.fr32[rk];
+            const float fv[3] = {f.x, f.y, f.z};
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                float v = S::sub(fv[r], cf[r]);
+                d[r] = S::sub(v, rintf(v));
+                lo[r] = max(-m, int32_t(ceilf(-reach[r] - d[r])));
+                hi[r] = min(m, int32_t(floorf(reach[r] - d[r])));
+            }
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_warp[wid] = __popc(bal);
+        // the same tests in both passes: first count, then (fill) write in image order
+        int32_t cnt = 0;
+        for (int32_t n2 = lo[2]; n2 <= hi[2]; ++n2)
+            for (int32_t n1 = lo[1]; n1 <= hi[1]; ++n1)
+                for (int32_t n0 = lo[0]; n0 <= hi[0]; ++n0) {
+                    const float e0 = S::add(d[0], float(n0)), e1 = S::add(d[1], float(n1)), e2 = S::add(d[2], float(n2));
+                    const float x = dot3s(Af[0], Af[3], Af[6], e0, e1, e2);
+                    const float y = dot3s(Af[1], Af[4], Af[7], e0, e1, e2);
+                    const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
+                    cnt += dot3s(x, y, z, x, y, z) <= R2f ? 1 : 0;
+                }
+        // ordered exclusive scan of the counts over the block
+        int32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[wid] = incl;
         __syncthreads();
         int32_t before = 0, tot = 0;
         for (int q = 0; q < 8; ++q) { int32_t v = s_warp[q]; if (q < wid) before += v; tot += v; }
-        if (FILL && keep) {
-            const int32_t pos = s_base + before + __popc(bal & ((1u << lane) - 1u));
-            if (pos < g.offsets[bin + 1]) {
-                // the stored position relative to the bin centre, in FP64 then rounded once
-                typedef St<double> S;
-                double d0 = S::sub(g.frac[3 * j], c[0]), d1 = S::sub(g.frac[3 * j + 1], c[1]),
-                       d2 = S::sub(g.frac[3 * j + 2], c[2]);
-                d0 = S::add(S::sub(d0, rint(d0)), double(n0));
-                d1 = S::add(S::sub(d1, rint(d1)), double(n1));
-                d2 = S::add(S::sub(d2, rint(d2)), double(n2));
-                const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
-                const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
-                const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
-                g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
-                g.type_out[pos] = g.types[j];
-                g.atom_out[pos] = j;
-            }
+        if (FILL && cnt > 0) {
+            int32_t pos = s_base + before + incl - cnt;
+            for (int32_t n2 = lo[2]; n2 <= hi[2]; ++n2)
+                for (int32_t n1 = lo[1]; n1 <= hi[1]; ++n1)
+                    for (int32_t n0 = lo[0]; n0 <= hi[0]; ++n0) {
+                        const float e0 = S::add(d[0], float(n0)), e1 = S::add(d[1], float(n1)),
+                                    e2 = S::add(d[2], float(n2));
+                        const float x = dot3s(Af[0], Af[3], Af[6], e0, e1, e2);
+                        const float y = dot3s(Af[1], Af[4], Af[7], e0, e1, e2);
+                        const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
+                        if (!(dot3s(x, y, z, x, y, z) <= R2f)) continue;
+                        if (pos < g.offsets[bin + 1]) {
+                            // the stored position relative to the bin centre, in FP64 then rounded once
+                            typedef St<double> D;
+                            double d0 = D::sub(g.frac[3 * j], c[0]), d1 = D::sub(g.frac[3 * j + 1], c[1]),
+                                   d2 = D::sub(g.frac[3 * j + 2], c[2]);
+                            d0 = D::add(D::sub(d0, rint(d0)), double(n0));
+                            d1 = D::add(D::sub(d1, rint(d1)), double(n1));
+                            d2 = D::add(D::sub(d2, rint(d2)), double(n2));
+                            const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
+                            const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
+                            const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
+                            g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
+                            g.type_out[pos] = g.types[j];
+                            g.atom_out[pos] = j;
+                        }
+                        ++pos;
+                    }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_base += tot;
