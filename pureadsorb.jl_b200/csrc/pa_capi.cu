@@ -72,6 +72,8 @@ struct pa_context {
     double* h_seg = nullptr;
     size_t h_seg_cap = 0;
     int32_t* h_cnt = nullptr;
+    char* h_stage = nullptr;  // pinned staging of batch uploads
+    size_t h_stage_cap = 0;
     std::vector<int64_t> up_seg_rng, up_sys_off;
     std::vector<int32_t> up_reach0;
     std::vector<unsigned char> up_rho2;
@@ -80,6 +82,7 @@ struct pa_context {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (h_seg) cudaFreeHost(h_seg);
         if (h_cnt) cudaFreeHost(h_cnt);
+        if (h_stage) cudaFreeHost(h_stage);
     }
 };
 
@@ -412,6 +415,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     B->nbins = bbase[nfw];
     // one packed upload of every table (and the list build's temporaries)
     Packer pk;
+    pk.host.reserve(size_t(1) << 16 | size_t(na) * 96 + size_t(nk) * 96 + size_t(B->nbins) * 8);
     Slots o{};
     o.framework_of = pk.add(fwo); o.cells = pk.add(cells); o.invcells = pk.add(inv); o.alphas = pk.add(alphas);
     o.const_offset = pk.add(co); o.atom_offsets = pk.add(B->atom_offsets); o.atoms = pk.add(atoms);
@@ -421,9 +425,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     const size_t t_q64 = pk.add(std::vector<double>(desc->charges, desc->charges + na));
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
     const bool lists = sizeof(F) == 4;
-    size_t t_frac = 0, t_q = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0, t_reach = 0, t_fr32 = 0;
+    size_t t_frac = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0, t_reach = 0, t_fr32 = 0;
     if (lists) {
-        std::vector<double> frac(3 * na), q(desc->charges, desc->charges + na);
+        std::vector<double> frac(3 * na);
         for (int fw = 0; fw < nfw; ++fw)
             for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
                 for (int r = 0; r < 3; ++r) {
@@ -450,11 +454,20 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         }
         t_order = pk.add(order);
         t_fr32 = pk.add(fr32);
-        t_frac = pk.add(frac); t_q = pk.add(q); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
+        t_frac = pk.add(frac); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
         t_nimg = pk.add(nimg); t_reach = pk.add(reach); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
     }
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.host.size(), st));
-    PA_CUDA(ctx, cudaMemcpyAsync(B->arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
+    // through the context's pinned staging buffer: the previous upload's copy out of it has
+    // finished (every upload waits on its stream before returning or before its list fill pass)
+    if (ctx->h_stage_cap < pk.host.size()) {
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr; ctx->h_stage_cap = 0;
+        PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), pk.host.size()));
+        ctx->h_stage_cap = pk.host.size();
+    }
+    std::memcpy(ctx->h_stage, pk.host.data(), pk.host.size());
+    PA_CUDA(ctx, cudaMemcpyAsync(B->arena, ctx->h_stage, pk.host.size(), cudaMemcpyHostToDevice, st));
     char* base = static_cast<char*>(B->arena);
     B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
     B->q64 = reinterpret_cast<const double*>(base + t_q64);
@@ -463,7 +476,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     if (lists) {
         // neighbour lists: count pass, padded offsets on the host, fill pass
         pa::ListGeom g{};
-        g.frac = reinterpret_cast<const double*>(base + t_frac); g.charges = reinterpret_cast<const double*>(base + t_q);
+        g.frac = reinterpret_cast<const double*>(base + t_frac); g.charges = reinterpret_cast<const double*>(base + t_q64);
         g.types = reinterpret_cast<const int32_t*>(base + o.types); g.cells = reinterpret_cast<const double*>(base + t_cells);
         g.atom_offsets = reinterpret_cast<const int32_t*>(base + o.atom_offsets);
         g.order = reinterpret_cast<const int32_t*>(base + t_order);

@@ -700,11 +700,12 @@ struct ListGeom {
 
 // Neighbour lists of the FP32 path: per bin, every atom image within R of the bin centre, in the
 // order (atom rank in `order`, image index) with the image index n0 + side (n1 + side n2) running
-// fastest. One thread per atom: an image can only lie within R if |d_r + n_r| <= R / L_r on each
-// axis (L_r the perpendicular width), so each thread tests only the images inside that box (a
-// margin far above FP32 rounding keeps every image the strict test would keep), then an ordered
-// block scan of the per-thread counts places its entries. Count and fill passes make the same
-// tests, so the fill writes exactly the counted entries.
+// fastest. Each thread takes LIST_ATOMS consecutive atom ranks. An image can only lie within R if
+// |d_r + n_r| <= R / L_r on each axis (L_r the perpendicular width), so a thread tests only the
+// images inside that box (a margin far above FP32 rounding keeps every image the strict test
+// would keep); an ordered block scan of the per-thread counts then places its entries. Count and
+// fill passes make the same tests, so the fill writes exactly the counted entries.
+#define LIST_ATOMS 4
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     __shared__ int32_t s_warp[8];
@@ -729,33 +730,44 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     typedef St<float> S;
-    for (int32_t r0 = a0; r0 < a1; r0 += blockDim.x) {
-        const int32_t rk = r0 + int32_t(threadIdx.x);
-        int32_t j = 0, lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
-        float d[3] = {0.f, 0.f, 0.f};
-        if (rk < a1) {
-            j = g.order[rk];
-            const float4 f = g.fr32[rk];
-            const float fv[3] = {f.x, f.y, f.z};
+    // strict FP32 membership of image (n0, n1, n2) of an atom at fractional offset d from the centre
+    const auto inside = [&](const float* d, int32_t n0, int32_t n1, int32_t n2) {
+        const float e0 = S::add(d[0], float(n0)), e1 = S::add(d[1], float(n1)), e2 = S::add(d[2], float(n2));
+        const float x = dot3s(Af[0], Af[3], Af[6], e0, e1, e2);
+        const float y = dot3s(Af[1], Af[4], Af[7], e0, e1, e2);
+        const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
+        return dot3s(x, y, z, x, y, z) <= R2f;
+    };
+    // LIST_ATOMS consecutive atom ranks per thread, their loads issued together
+    for (int32_t r0 = a0; r0 < a1; r0 += LIST_ATOMS * int32_t(blockDim.x)) {
+        int32_t j[LIST_ATOMS], lo[LIST_ATOMS][3], hi[LIST_ATOMS][3];
+        float d[LIST_ATOMS][3];
+        int32_t cnt = 0;
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                float v = S::sub(fv[r], cf[r]);
-                d[r] = S::sub(v, rintf(v));
-                lo[r] = max(-m, int32_t(ceilf(-reach[r] - d[r])));
-                hi[r] = min(m, int32_t(floorf(reach[r] - d[r])));
+        for (int u = 0; u < LIST_ATOMS; ++u) {
+            const int32_t rk = r0 + LIST_ATOMS * int32_t(threadIdx.x) + u;
+            j[u] = 0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) { lo[u][r] = 0; hi[u][r] = -1; d[u][r] = 0.f; }
+            if (rk < a1) {
+                j[u] = g.order[rk];
+                const float4 f = g.fr32[rk];
+                const float fv[3] = {f.x, f.y, f.z};
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    float v = S::sub(fv[r], cf[r]);
+                    d[u][r] = S::sub(v, rintf(v));
+                    lo[u][r] = max(-m, int32_t(ceilf(-reach[r] - d[u][r])));
+                    hi[u][r] = min(m, int32_t(floorf(reach[r] - d[u][r])));
+                }
             }
         }
-        // the same tests in both passes: first count, then (fill) write in image order
-        int32_t cnt = 0;
-        for (int32_t n2 = lo[2]; n2 <= hi[2]; ++n2)
-            for (int32_t n1 = lo[1]; n1 <= hi[1]; ++n1)
-                for (int32_t n0 = lo[0]; n0 <= hi[0]; ++n0) {
-                    const float e0 = S::add(d[0], float(n0)), e1 = S::add(d[1], float(n1)), e2 = S::add(d[2], float(n2));
-                    const float x = dot3s(Af[0], Af[3], Af[6], e0, e1, e2);
-                    const float y = dot3s(Af[1], Af[4], Af[7], e0, e1, e2);
-                    const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
-                    cnt += dot3s(x, y, z, x, y, z) <= R2f ? 1 : 0;
-                }
+        // the same tests in both passes: first count, then (fill) write in (rank, image) order
+#pragma unroll
+        for (int u = 0; u < LIST_ATOMS; ++u)
+            for (int32_t n2 = lo[u][2]; n2 <= hi[u][2]; ++n2)
+                for (int32_t n1 = lo[u][1]; n1 <= hi[u][1]; ++n1)
+                    for (int32_t n0 = lo[u][0]; n0 <= hi[u][0]; ++n0) cnt += inside(d[u], n0, n1, n2) ? 1 : 0;
         // ordered exclusive scan of the counts over the block
         int32_t incl = cnt;
 #pragma unroll
@@ -769,32 +781,30 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         for (int q = 0; q < 8; ++q) { int32_t v = s_warp[q]; if (q < wid) before += v; tot += v; }
         if (FILL && cnt > 0) {
             int32_t pos = s_base + before + incl - cnt;
-            for (int32_t n2 = lo[2]; n2 <= hi[2]; ++n2)
-                for (int32_t n1 = lo[1]; n1 <= hi[1]; ++n1)
-                    for (int32_t n0 = lo[0]; n0 <= hi[0]; ++n0) {
-                        const float e0 = S::add(d[0], float(n0)), e1 = S::add(d[1], float(n1)),
-                                    e2 = S::add(d[2], float(n2));
-                        const float x = dot3s(Af[0], Af[3], Af[6], e0, e1, e2);
-                        const float y = dot3s(Af[1], Af[4], Af[7], e0, e1, e2);
-                        const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
-                        if (!(dot3s(x, y, z, x, y, z) <= R2f)) continue;
-                        if (pos < g.offsets[bin + 1]) {
-                            // the stored position relative to the bin centre, in FP64 then rounded once
-                            typedef St<double> D;
-                            double d0 = D::sub(g.frac[3 * j], c[0]), d1 = D::sub(g.frac[3 * j + 1], c[1]),
-                                   d2 = D::sub(g.frac[3 * j + 2], c[2]);
-                            d0 = D::add(D::sub(d0, rint(d0)), double(n0));
-                            d1 = D::add(D::sub(d1, rint(d1)), double(n1));
-                            d2 = D::add(D::sub(d2, rint(d2)), double(n2));
-                            const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
-                            const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
-                            const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
-                            g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[j]));
-                            g.type_out[pos] = g.types[j];
-                            g.atom_out[pos] = j;
+#pragma unroll
+            for (int u = 0; u < LIST_ATOMS; ++u)
+                for (int32_t n2 = lo[u][2]; n2 <= hi[u][2]; ++n2)
+                    for (int32_t n1 = lo[u][1]; n1 <= hi[u][1]; ++n1)
+                        for (int32_t n0 = lo[u][0]; n0 <= hi[u][0]; ++n0) {
+                            if (!inside(d[u], n0, n1, n2)) continue;
+                            if (pos < g.offsets[bin + 1]) {
+                                // the stored position relative to the bin centre, in FP64 then rounded once
+                                typedef St<double> D;
+                                const int32_t ja = j[u];
+                                double d0 = D::sub(g.frac[3 * ja], c[0]), d1 = D::sub(g.frac[3 * ja + 1], c[1]),
+                                       d2 = D::sub(g.frac[3 * ja + 2], c[2]);
+                                d0 = D::add(D::sub(d0, rint(d0)), double(n0));
+                                d1 = D::add(D::sub(d1, rint(d1)), double(n1));
+                                d2 = D::add(D::sub(d2, rint(d2)), double(n2));
+                                const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
+                                const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
+                                const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
+                                g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[ja]));
+                                g.type_out[pos] = g.types[ja];
+                                g.atom_out[pos] = ja;
+                            }
+                            ++pos;
                         }
-                        ++pos;
-                    }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_base += tot;
