@@ -152,17 +152,39 @@ cudaError_t upload_cached(DevMem& m, std::vector<T>& cache, const std::vector<T>
 
 // Host staging of many small device tables into one buffer (256-byte aligned slots), uploaded
 // with a single copy into one allocation.
+// Packs the tables of one upload into the context's pinned staging buffer (256-byte aligned slots),
+// from which one copy moves them to the device. The buffer only grows; a previous upload's copy out
+// of it has always finished (every upload waits on its stream before its list fill pass or its
+// return, and a failed upload synchronises).
 struct Packer {
-    std::vector<char> host;
+    pa_context* ctx;
+    size_t n = 0;
+    bool ok = true;
+    explicit Packer(pa_context* c) : ctx(c) {}
+    bool grow(size_t need) {
+        if (need <= ctx->h_stage_cap) return true;
+        const size_t cap = std::max(need, std::max(2 * ctx->h_stage_cap, size_t(1) << 20));
+        char* p = nullptr;
+        if (cudaMallocHost(reinterpret_cast<void**>(&p), cap) != cudaSuccess) { ok = false; return false; }
+        if (n) std::memcpy(p, ctx->h_stage, n);
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = p;
+        ctx->h_stage_cap = cap;
+        return true;
+    }
     template <typename T> size_t add(const std::vector<T>& v) {
-        size_t off = (host.size() + 255) & ~size_t(255);
-        host.resize(off + std::max<size_t>(v.size() * sizeof(T), 16));
-        if (!v.empty()) std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        const size_t off = (n + 255) & ~size_t(255), bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+        if (!grow(off + bytes)) return 0;
+        if (!v.empty()) std::memcpy(ctx->h_stage + off, v.data(), v.size() * sizeof(T));
+        n = off + bytes;
         return off;
     }
     size_t reserve(size_t bytes) {
-        size_t off = (host.size() + 255) & ~size_t(255);
-        host.resize(off + std::max<size_t>(bytes, 16), 0);
+        const size_t off = (n + 255) & ~size_t(255);
+        bytes = std::max<size_t>(bytes, 16);
+        if (!grow(off + bytes)) return 0;
+        std::memset(ctx->h_stage + off, 0, bytes);
+        n = off + bytes;
         return off;
     }
 };
@@ -414,8 +436,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     }
     B->nbins = bbase[nfw];
     // one packed upload of every table (and the list build's temporaries)
-    Packer pk;
-    pk.host.reserve(size_t(1) << 16 | size_t(na) * 96 + size_t(nk) * 96 + size_t(B->nbins) * 8);
+    Packer pk(ctx);
     Slots o{};
     o.framework_of = pk.add(fwo); o.cells = pk.add(cells); o.invcells = pk.add(inv); o.alphas = pk.add(alphas);
     o.const_offset = pk.add(co); o.atom_offsets = pk.add(B->atom_offsets); o.atoms = pk.add(atoms);
@@ -457,17 +478,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         t_frac = pk.add(frac); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
         t_nimg = pk.add(nimg); t_reach = pk.add(reach); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
     }
-    PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.host.size(), st));
-    // through the context's pinned staging buffer: the previous upload's copy out of it has
-    // finished (every upload waits on its stream before returning or before its list fill pass)
-    if (ctx->h_stage_cap < pk.host.size()) {
-        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
-        ctx->h_stage = nullptr; ctx->h_stage_cap = 0;
-        PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), pk.host.size()));
-        ctx->h_stage_cap = pk.host.size();
-    }
-    std::memcpy(ctx->h_stage, pk.host.data(), pk.host.size());
-    PA_CUDA(ctx, cudaMemcpyAsync(B->arena, ctx->h_stage, pk.host.size(), cudaMemcpyHostToDevice, st));
+    if (!pk.ok) return fail(ctx, PA_ERR_CUDA, "pinned staging allocation failed");
+    PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.n, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(B->arena, ctx->h_stage, pk.n, cudaMemcpyHostToDevice, st));
     char* base = static_cast<char*>(B->arena);
     B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
     B->q64 = reinterpret_cast<const double*>(base + t_q64);

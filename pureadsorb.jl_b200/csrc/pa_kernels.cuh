@@ -717,10 +717,10 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     const double c[3] = {double(__fdiv_rn(float(bx) + 0.5f, float(nb[0]))),
                          double(__fdiv_rn(float(by) + 0.5f, float(nb[1]))),
                          double(__fdiv_rn(float(bz) + 0.5f, float(nb[2])))};
-    const double* A = g.cells + 9 * fw;
+    double A[9];
     float Af[9];
 #pragma unroll
-    for (int r = 0; r < 9; ++r) Af[r] = float(A[r]);
+    for (int r = 0; r < 9; ++r) { A[r] = g.cells[9 * fw + r]; Af[r] = float(A[r]); }
     const float cf[3] = {float(c[0]), float(c[1]), float(c[2])};
     const float R2f = float(g.radius2[fw]);
     const float reach[3] = {g.reach[3 * fw], g.reach[3 * fw + 1], g.reach[3 * fw + 2]};
@@ -781,30 +781,36 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         for (int q = 0; q < 8; ++q) { int32_t v = s_warp[q]; if (q < wid) before += v; tot += v; }
         if (FILL && cnt > 0) {
             int32_t pos = s_base + before + incl - cnt;
+            const int32_t pend = g.offsets[bin + 1];
+            typedef St<double> D;
 #pragma unroll
-            for (int u = 0; u < LIST_ATOMS; ++u)
+            for (int u = 0; u < LIST_ATOMS; ++u) {
+                if (lo[u][0] > hi[u][0] || lo[u][1] > hi[u][1] || lo[u][2] > hi[u][2]) continue;
+                // the atom's FP64 offset from the bin centre, its charge and type: read once
+                const int32_t ja = j[u];
+                double b0 = D::sub(g.frac[3 * ja], c[0]), b1 = D::sub(g.frac[3 * ja + 1], c[1]),
+                       b2 = D::sub(g.frac[3 * ja + 2], c[2]);
+                b0 = D::sub(b0, rint(b0)); b1 = D::sub(b1, rint(b1)); b2 = D::sub(b2, rint(b2));
+                const float qa = float(g.charges[ja]);
+                const int32_t ta = g.types[ja];
                 for (int32_t n2 = lo[u][2]; n2 <= hi[u][2]; ++n2)
                     for (int32_t n1 = lo[u][1]; n1 <= hi[u][1]; ++n1)
                         for (int32_t n0 = lo[u][0]; n0 <= hi[u][0]; ++n0) {
                             if (!inside(d[u], n0, n1, n2)) continue;
-                            if (pos < g.offsets[bin + 1]) {
+                            if (pos < pend) {
                                 // the stored position relative to the bin centre, in FP64 then rounded once
-                                typedef St<double> D;
-                                const int32_t ja = j[u];
-                                double d0 = D::sub(g.frac[3 * ja], c[0]), d1 = D::sub(g.frac[3 * ja + 1], c[1]),
-                                       d2 = D::sub(g.frac[3 * ja + 2], c[2]);
-                                d0 = D::add(D::sub(d0, rint(d0)), double(n0));
-                                d1 = D::add(D::sub(d1, rint(d1)), double(n1));
-                                d2 = D::add(D::sub(d2, rint(d2)), double(n2));
+                                const double d0 = D::add(b0, double(n0)), d1 = D::add(b1, double(n1)),
+                                             d2 = D::add(b2, double(n2));
                                 const double dx = dot3s(A[0], A[3], A[6], d0, d1, d2);
                                 const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
                                 const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
-                                g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), float(g.charges[ja]));
-                                g.type_out[pos] = g.types[ja];
+                                g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), qa);
+                                g.type_out[pos] = ta;
                                 g.atom_out[pos] = ja;
                             }
                             ++pos;
                         }
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_base += tot;
