@@ -244,6 +244,8 @@ typedef struct pa_grad_sums {
     double* s_guest;     /* optional, 2*Σ_s nk(framework_of[s]): Σ_i w_i S_g,i(k) (re, im)      */
     double window;       /* in: selection window in units of kT (0: 50)                         */
     int64_t recomputed;  /* out: insertions the adjoint pass recomputed                         */
+    int32_t lj_only;     /* in: nonzero skips the charge derivatives (d_charge and s_guest are
+                            returned as zeros), for callers that only need ε and σ               */
 } pa_grad_sums;
 
 /* pa_widom plus the adjoint sums. FP32 batches only (the adjoint walks the FP32 path's bins and

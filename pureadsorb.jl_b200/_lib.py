@@ -61,7 +61,7 @@ class Tuning(ctypes.Structure):
 
 class GradSums(ctypes.Structure):
     _fields_ = [("xmax", _p), ("sum_w", _p), ("d_epsilon", _p), ("d_sigma", _p), ("d_charge", _p),
-                ("s_guest", _p), ("window", _f64), ("recomputed", _i64)]
+                ("s_guest", _p), ("window", _f64), ("recomputed", _i64), ("lj_only", _i32)]
 
 
 # (name, restype, argtypes): every entry point the header declares

@@ -798,8 +798,12 @@ pa_status pa_batch_hardcore_bounds(pa_context* ctx, const pa_batch* B, double* b
     if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
     const int N = B->nguest, nt = B->ntypes, nfw = B->nfw;
-    // [site sigma N*nt][site eps N*nt][guest charges N][bounds nfw][error flag]
-    std::vector<double> h(2 * N * nt + N + nfw + 1, 0.0);
+    // [site sigma N*nt][site eps N*nt][guest charges N][error flag][chunk sums nfw*nchunk]
+    int64_t amax = 0;
+    for (int f = 0; f < nfw; ++f) amax = std::max<int64_t>(amax, B->atom_offsets[f + 1] - B->atom_offsets[f]);
+    const int32_t nchunk = int32_t(std::max<int64_t>(1, (amax * N + BOUND_CHUNK - 1) / BOUND_CHUNK));
+    if (nfw > 65535) return fail(ctx, PA_ERR_ARG, "pa_batch_hardcore_bounds supports at most 65535 frameworks");
+    std::vector<double> h(2 * N * nt + N + 1 + int64_t(nfw) * nchunk, 0.0);
     std::copy(B->site_sigma.begin(), B->site_sigma.end(), h.begin());
     std::copy(B->site_eps.begin(), B->site_eps.end(), h.begin() + N * nt);
     std::copy(B->guest_q.begin(), B->guest_q.end(), h.begin() + 2 * N * nt);
@@ -814,20 +818,25 @@ pa_status pa_batch_hardcore_bounds(pa_context* ctx, const pa_batch* B, double* b
     g.atom_offsets = B->precision == PA_PRECISION_F32 ? v32.atom_offsets : v64.atom_offsets;
     g.alphas = B->precision == PA_PRECISION_F32 ? v32.alphas : v64.alphas;
     g.site_sig = d; g.site_eps = d + N * nt; g.gq = d + 2 * N * nt; g.N = N; g.nt = nt; g.r_lj = B->cutoff;
-    g.out = d + 2 * N * nt + N;
-    g.err = reinterpret_cast<int32_t*>(d + 2 * N * nt + N + nfw);
-    pa::k_hardcore_bound<<<unsigned(nfw), 256, 0, st>>>(g);
+    g.err = reinterpret_cast<int32_t*>(d + 2 * N * nt + N);
+    g.out = d + 2 * N * nt + N + 1;
+    g.nchunk = nchunk;
+    pa::k_hardcore_bound<<<dim3(unsigned(nchunk), unsigned(nfw)), 256, 0, st>>>(g);
     PA_CUDA(ctx, cudaGetLastError());
-    std::vector<double> out(nfw + 1);
-    PA_CUDA(ctx, cudaMemcpyAsync(out.data(), g.out, sizeof(double) * (nfw + 1), cudaMemcpyDeviceToHost, st));
+    std::vector<double> out(1 + int64_t(nfw) * nchunk);
+    PA_CUDA(ctx, cudaMemcpyAsync(out.data(), d + 2 * N * nt + N, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
     pa_status ws = wait_stream(ctx);
     if (ws != PA_OK) return ws;
     int32_t e = 0;
-    std::memcpy(&e, &out[nfw], sizeof(int32_t));
+    std::memcpy(&e, &out[0], sizeof(int32_t));
     if (e) return fail(ctx, PA_ERR_ARG, "hard-core bound: a root search (find_r0) failed");
     double qabs = 0;
     for (double q : B->guest_q) qabs += std::fabs(q);
-    for (int f = 0; f < nfw; ++f) bs[f] = out[f] + 2 * pa::KE * qabs * B->recip_bound[f];
+    for (int f = 0; f < nfw; ++f) {
+        double sfw = 0.0;  // the chunks in order
+        for (int32_t c = 0; c < nchunk; ++c) sfw += out[1 + int64_t(f) * nchunk + c];
+        bs[f] = sfw + 2 * pa::KE * qabs * B->recip_bound[f];
+    }
     return PA_OK;
 }
 
@@ -1206,6 +1215,7 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
     g.heavy = ctx->heavy.as<int32_t>(); g.nheavy = ctx->counters.as<int32_t>() + 4;
     g.g_w = ctx->g_w.as<double>(); g.g_lj = ctx->g_lj.as<double>(); g.g_q = ctx->g_q.as<double>();
     g.g_k = ctx->g_k.as<double>(); g.frac = B->frac64; g.kpref2 = B->kpref2;
+    g.lj_only = grad->lj_only != 0 ? 1 : 0;
     {
         Timer tm(ctx, 5);
         pa::k_heavy<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, ca, g);
@@ -1214,7 +1224,7 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
         PA_DISPATCH_NS(N, (e = launch_grad<NSV>(B, ca, w, g, ctx->num_sms, st)));
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("adjoint kernel launch: ") + cudaGetErrorString(e));
         int nl = 2;
-        if (B->nk > 0) {
+        if (B->nk > 0 && !g.lj_only) {
             int32_t amax = 0;
             for (int fw = 0; fw < B->nfw; ++fw) amax = std::max(amax, B->atom_offsets[fw + 1] - B->atom_offsets[fw]);
             if (amax > 0 && nsys <= 65535) {
@@ -1230,9 +1240,9 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
     std::vector<double> glj(nlj);
     int32_t nh = 0;
     PA_CUDA(ctx, cudaMemcpyAsync(glj.data(), ctx->g_lj.p, sizeof(double) * nlj, cudaMemcpyDeviceToHost, st));
-    if (aoff[nsys] > 0)
+    if (aoff[nsys] > 0 && !g.lj_only)
         PA_CUDA(ctx, cudaMemcpyAsync(grad->d_charge, ctx->g_q.p, sizeof(double) * aoff[nsys], cudaMemcpyDeviceToHost, st));
-    if (grad->s_guest && koff[nsys] > 0)
+    if (grad->s_guest && koff[nsys] > 0 && !g.lj_only)
         PA_CUDA(ctx, cudaMemcpyAsync(grad->s_guest, ctx->g_k.p, sizeof(double) * 2 * koff[nsys], cudaMemcpyDeviceToHost, st));
     PA_CUDA(ctx, cudaMemcpyAsync(&nh, ctx->counters.as<int32_t>() + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     pa_status ws = wait_stream(ctx);

@@ -24,6 +24,7 @@ struct GradArgs {
     const int64_t* sys_aoff;  // nsys+1: each system's first per-atom slot
     const int64_t* sys_koff;  // nsys+1: each system's first k slot
     int32_t nsys;
+    int32_t lj_only;          // nonzero: no charge derivatives (real-space terms, G_k)
     int32_t* heavy;           // n_act: local indices of the recomputed insertions
     int32_t* nheavy;          // count of heavy
     double* g_w;              // nsys: Σ w over the recomputed insertions
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
         gqs[s] = b.gq[s];
         gsb[3 * s] = b.gsite[3 * s]; gsb[3 * s + 1] = b.gsite[3 * s + 1]; gsb[3 * s + 2] = b.gsite[3 * s + 2];
     }
-    const bool charged = b.has_charge != 0;
+    const bool charged = b.has_charge != 0 && g.lj_only == 0;
     const int32_t nh = *g.nheavy;
     const int32_t nwarps = gridDim.x * PA_WARPSG;
     const float NLOG2E = -1.4426950408889634f;

@@ -872,9 +872,11 @@ struct BoundArgs {
     const double* gq;        // N guest charges
     int32_t N, nt;
     double r_lj;
-    double* out;             // nfw
+    double* out;             // nfw*nchunk: partial sum of each chunk of BOUND_CHUNK (site, atom) pairs
+    int32_t nchunk;          // chunks per framework (the largest framework's count)
     int32_t* err;
 };
+#define BOUND_CHUNK 2048
 
 __device__ __forceinline__ double bound_pair_energy(double r, double s, double e, double K, double alpha) {
     double x = (s * s) / (r * r);
@@ -901,15 +903,23 @@ __device__ double bound_find_r0(double s, double e, double K, double alpha, doub
     return fmin((lo + hi) / 2, r_lj);
 }
 
+// One CTA per chunk of BOUND_CHUNK (site, atom) pairs of one framework (blockIdx.y), so that a
+// large framework's root searches spread over the GPU; the host adds the chunks' partial sums in
+// chunk order.
 __global__ void __launch_bounds__(256) k_hardcore_bound(BoundArgs g) {
     __shared__ double s_red[256];
-    const int32_t fw = blockIdx.x;
+    const int32_t fw = blockIdx.y, ch = blockIdx.x;
     const int32_t a0 = g.atom_offsets[fw], a1 = g.atom_offsets[fw + 1];
     const double alpha = g.alphas[fw];
     const int64_t npair = int64_t(a1 - a0) * g.N;
+    const int64_t p0 = int64_t(ch) * BOUND_CHUNK, p1 = min(npair, p0 + BOUND_CHUNK);
+    if (p0 >= npair) {
+        if (threadIdx.x == 0) g.out[int64_t(fw) * g.nchunk + ch] = 0.0;
+        return;
+    }
     double acc = 0.0;
     int32_t lerr = 0;
-    for (int64_t p = threadIdx.x; p < npair; p += blockDim.x) {
+    for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const int32_t a = int32_t(p / (a1 - a0)), j = a0 + int32_t(p % (a1 - a0));
         const int32_t t = g.types[j];
         const double e = g.site_eps[a * g.nt + t], s = g.site_sig[a * g.nt + t];
@@ -931,7 +941,7 @@ __global__ void __launch_bounds__(256) k_hardcore_bound(BoundArgs g) {
         if (int(threadIdx.x) < w) s_red[threadIdx.x] += s_red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) g.out[fw] = s_red[0];
+    if (threadIdx.x == 0) g.out[int64_t(fw) * g.nchunk + ch] = s_red[0];
 }
 
 }  // namespace pa

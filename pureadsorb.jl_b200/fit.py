@@ -75,7 +75,7 @@ def fit_lj_scales(batch, guest, ff, types, targets, *, T, ninsert, steps=200, lr
         ffx = scaled_forcefield(ff, types, x)
         b = b.with_forcefield(ffx, move_device=True, device_bounds=True)
         lnk, grads = widom_grad(b, guest, ffx, T=T, ninsert=ninsert, backend=backend, seed=seed, nblocks=nblocks,
-                                reduce=False)
+                                reduce=False, charges=False)
         use = np.isfinite(lnk) & np.isfinite(targets)
         r = (lnk - targets)[use]
         g_eps = np.array([g.epsilon[idx] for g, u in zip(grads, use) if u]) * eps0[idx]

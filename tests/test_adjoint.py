@@ -131,3 +131,39 @@ def test_untouched_types_have_zero_gradient(case, adjoint):
     # every type of the force field appears in the batch, so all gradients are finite
     assert np.all(np.isfinite(g.epsilon)) and np.all(np.isfinite(g.sigma)) and np.all(np.isfinite(g.charges))
     assert g.sum_w > 0 and sums["sum_w"] == g.sum_w
+
+
+def test_assemble_all_equals_per_system_chain_rule(pa):
+    """The vectorised host assembly of the gradients (every system at once) against the per-system
+    composition of the device-sum mapping, tail_delta_pair_grad and pair_to_type_grad, on a batch of
+    several frameworks with synthetic adjoint sums."""
+    fws, ff, guest, ewald, _ = pa.synthetic.batched(nfw=4, T=np.float64, max_unit_atoms=120)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald)
+    rng = np.random.default_rng(3)
+    N, nt = len(b.guest_types), len(b.sigma)
+    nat, _ = pa.adjoint.system_offsets(b)
+    sums = [dict(xmax=rng.normal(), sum_w=rng.uniform(1, 2), d_epsilon=rng.normal(size=N * nt),
+                 d_sigma=rng.normal(size=N * nt), d_charge=rng.normal(size=int(nat[s])), recomputed=s)
+            for s in range(b.nsys)]
+    kT = 0.0257
+    got = pa.adjoint.assemble_all(b, ff, sums, kT)
+    nff = len(ff.names)
+    c2o = np.asarray(b.compact_to_orig) - 1
+    gt = np.asarray(b.guest_types) - 1
+    for s in range(b.nsys):
+        p = sums[s]
+        dS, dE = np.zeros((nff, nff)), np.zeros((nff, nff))
+        for a in range(N):
+            dE[c2o[gt[a]], c2o] += p["d_epsilon"].reshape(N, nt)[a] / p["sum_w"]
+            dS[c2o[gt[a]], c2o] += p["d_sigma"].reshape(N, nt)[a] / p["sum_w"]
+        fw = b.framework_of[s] - 1
+        a0, a1 = b.atom_offsets[fw], b.atom_offsets[fw + 1]
+        counts = np.bincount(c2o[np.asarray(b.types[a0:a1]) - 1], minlength=nff)
+        gc = np.bincount(np.asarray(b.guest_types_orig) - 1, minlength=nff)
+        tS, tE = pa.forcefield.tail_delta_pair_grad(ff, counts, gc, b.volumes[fw])
+        g_sig, g_eps = pa.forcefield.pair_to_type_grad(ff, dS + tS, dE + tE)
+        ok = np.isfinite(g_eps)
+        assert np.allclose(got[s].epsilon[ok], -g_eps[ok] / kT, rtol=1e-12, atol=0)
+        assert np.array_equal(np.isfinite(got[s].epsilon), ok)
+        assert np.allclose(got[s].sigma, -g_sig / kT, rtol=1e-12, atol=1e-300)
+        assert got[s].charges.shape == (a1 - a0,) and got[s].recomputed == s

@@ -104,3 +104,18 @@ def test_fp64_batch_is_refused(pa, backend, case):
     b64 = case.batch(T=np.float64)
     with pytest.raises(Exception, match="PA_PRECISION_F32"):
         _device(pa, backend, case, b64)
+
+
+def test_lj_only_mode_keeps_lj_gradients(pa, backend, case):
+    """charges=False skips the device's charge terms: the ε and σ derivatives are those of the full
+    adjoint (to the rounding of their atomic accumulation order), and no charge gradient is made."""
+    b32 = case.batch(T=np.float32)
+    full, gf = _device(pa, backend, case, b32)
+    lj, gl = pa.widom_grad(b32, case.guest, case.ff, T=298.15, ninsert=NINS, backend=backend, seed=SEED,
+                           nblocks=NBLOCKS, run=RUN, charges=False)
+    assert gl[0].charges is None
+    assert gl[0].recomputed == gf[0].recomputed
+    assert lj[0].K_H == full[0].K_H
+    for name in ("epsilon", "sigma"):
+        a, f = getattr(gl[0], name), getattr(gf[0], name)
+        assert np.max(np.abs(a - f)) <= 1e-9 * np.max(np.abs(f)), name
