@@ -142,6 +142,24 @@ pa_status pa_batch_info(const pa_batch* batch, int64_t* list_entries, int64_t* n
  * (src/widom.jl:202-253): rho2 is nsys*N*nt (system s, site a, type t at
  * (s-1)*N*nt + (a-1)*nt + t, 1-based), reach0 is 3*nsys. With reject = 0 they may be NULL and
  * every insertion's energy is computed (`widom_singlephase`, src/widom.jl:296). */
+/* A loaded configuration to insert into: Widom along an NVT chain (`widom_chain_kernel!`,
+ * src/nvt.jl:85-124; the configuration as `SystemState` holds it, src/state.jl:5-126). Each test
+ * insertion sees the host and every live guest of its system: host-guest real space, the
+ * reciprocal cross term against the system's running structure factor (host plus guests, replacing
+ * the host's), guest-guest real space (each site pair its own minimum image, src/guest.jl:51-75),
+ * and the system's pose-independent term (`insertion_constant_term`, src/nvt.jl:45-66) in place of
+ * the framework's constant offset. Needs an FP32 batch with one framework per system
+ * (framework_of[s] == s + 1) and a single-phase call (reject = 0). */
+typedef struct pa_chain_args {
+    const double* Sk;             /* 2*nk (re, im): each system's running S(k) over its k table */
+    const double* const_term;     /* nsys: each system's pose-independent term (eV)             */
+    const int32_t* guest_offsets; /* nsys+1: the live guests of system s are
+                                     [guest_offsets[s], guest_offsets[s+1])                    */
+    const double* guest_sites;    /* 3*N per live guest, guest-major: Cartesian site positions */
+    int64_t k_offset;             /* added to every insertion's per-system index: the cycle's
+                                     insertions follow the previous cycles' in the pose stream  */
+} pa_chain_args;
+
 typedef struct pa_widom_args {
     double kT;          /* eV, already rounded to the batch's float type by the caller */
     int64_t ninsert;
@@ -156,6 +174,7 @@ typedef struct pa_widom_args {
      * per-system sample order); segment_end <= 0 means "to the end". */
     int64_t segment_begin;
     int64_t segment_end;
+    const pa_chain_args* chain;  /* optional (NULL: insertion into the empty framework) */
 } pa_widom_args;
 
 #define PA_SEGMENT 2048

@@ -921,6 +921,41 @@ void or_insertion_energy(const or_batch_view* b, int32_t fw, int64_t n, const do
     for (int64_t i = 0; i < n; ++i) out[i] = insertion_energy(*b, fw, pos + 3 * i, quat + 4 * i, nullptr, nullptr);
 }
 
+// widom_chain_kernel!'s energy (src/nvt.jl:85-124) of explicit poses of one system, without its
+// constant term: insertion_energy against the view's k table and structure factor (the caller's
+// view carries the system's running S(k), host plus guests, in place of Shost), plus the
+// guest-guest real space over the system's live guests (src/guest.jl:51-75: every site pair its
+// own minimum image, LJ inside the LJ cutoff, q_a q_b erfc(alpha r)/r inside the Ewald cutoff).
+// gsites: 3*N per live guest, guest-major, Cartesian.
+void or_chain_energy(const or_batch_view* bp, int32_t fw, int64_t n, const double* pos, const double* quat, int64_t ng,
+                     const double* gsites, double* out) {
+    const or_batch_view& b = *bp;
+    const int N = b.nguest, nt = b.ntypes;
+    const double* A = b.cells + 9 * fw; const double* invA = b.invcells + 9 * fw;
+    const double rl2 = b.cutoff * b.cutoff, re2 = b.ewald_cutoff * b.ewald_cutoff, alpha = b.alphas[fw];
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const double* p = pos + 3 * i; const double* q = quat + 4 * i;
+        double e = insertion_energy(b, fw, p, q, nullptr, nullptr);
+        double gs[3 * 16];
+        for (int a = 0; a < N; ++a) rotate_strict<double>(q, b.guest_sites + 3 * a, gs + 3 * a);
+        double Elj = 0, Esr = 0;
+        for (int64_t j = 0; j < ng; ++j)
+            for (int a = 0; a < N; ++a)
+                for (int c = 0; c < N; ++c) {
+                    const double* o = gsites + 3 * (j * N + c);
+                    double D[3] = {p[0] + gs[3 * a] - o[0], p[1] + gs[3 * a + 1] - o[1], p[2] + gs[3 * a + 2] - o[2]};
+                    minimum_image_strict<double>(A, invA, D);
+                    const double r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+                    if (!(r2 < rl2 || r2 < re2)) continue;
+                    const int ta = b.guest_types[a] - 1, tc = b.guest_types[c] - 1;
+                    if (r2 < rl2) Elj += lj_pair(r2, b.sigma[ta + nt * tc], b.epsilon[ta + nt * tc]);
+                    if (r2 < re2) { const double r = std::sqrt(r2); Esr += b.guest_charges[a] * b.guest_charges[c] * std::erfc(alpha * r) / r; }
+                }
+        out[i] = e + Elj + KE * Esr;
+    }
+}
+
 // insertion_energy_reference (src/reference.jl:31-67): per-site minimum image, erfc, and the full
 // k set with both the cross and the guest self term. hpos/htype(1-based)/hq are the host atoms.
 double or_insertion_energy_reference(const double* pos, const double* q, int32_t N, const double* gsites,

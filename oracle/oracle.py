@@ -65,6 +65,7 @@ def lib():
             "or_widom": (ctypes.c_int, [ctypes.POINTER(BatchView), _i32, _f64, _i64, _u64, _i32, _i64, _i32, _p, _p,
                                         _p, _p, _p, _p, _p, _p, _p, _i32]),
             "or_insertion_energy": (None, [ctypes.POINTER(BatchView), _i32, _i64, _p, _p, _p]),
+            "or_chain_energy": (None, [ctypes.POINTER(BatchView), _i32, _i64, _p, _p, _i64, _p, _p]),
             "or_insertion_energy_reference": (_f64, [_p, _p, _i32, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i64, _p,
                                                      _p, _p, _p, _f64, _i64, _p, _p, _p]),
             "or_hardcore_flags": (None, [ctypes.POINTER(BatchView), _i32, _i32, _i64, _p, _p, _p, _p, _i32, _p]),
@@ -302,4 +303,16 @@ def hardcore_flags(v, precision, s, rpos, quat, rho2, reach0, brute=False):
     n = len(rpos) // 3
     out = np.zeros(n, np.uint8)
     lib().or_hardcore_flags(ctypes.byref(v), precision, s, n, P(rpos), P(quat), P(r2), P(r0), int(brute), P(out))
+    return out
+
+
+def chain_energy(v, fw, pos, quat, gsites):
+    """widom_chain_kernel!'s energy without the constant term at explicit poses of system fw (the
+    view's Shost being that system's running S(k)); gsites: the live guests' sites (ng, N, 3)."""
+    pos, quat = c64(np.asarray(pos).reshape(-1)), c64(np.asarray(quat).reshape(-1))
+    g = c64(np.asarray(gsites).reshape(-1)) if np.asarray(gsites).size else c64(np.zeros(3))
+    ng = int(np.asarray(gsites).size // (3 * v.nguest))
+    n = len(pos) // 3
+    out = np.zeros(n)
+    lib().or_chain_energy(ctypes.byref(v), fw, n, P(pos), P(quat), ng, P(g), P(out))
     return out

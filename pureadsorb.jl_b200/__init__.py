@@ -16,8 +16,11 @@ from . import adjoint
 from .adjoint import WidomGrad, fold_replicas, widom_grad
 from .tune import TuneReport, autotune
 from . import fit
+from . import chain
+from .chain import SystemState, insertion_constant_term, widom_along_chain, widom_chain
 from .widom import (B200Backend, WidomResult, _reduce, _widom, block_sums, boltzmann_weight, build_rejection_tables,
                     default_run, sys_of_index, system_counts, widom, widom_singlephase)
 
 __all__ = ["Framework", "read_cif", "replicate", "ForceField", "read_forcefield", "Guest", "read_guest",
-           "EwaldParams", "FrameworkBatch", "widom", "WidomResult", "B200Backend", "widom_grad", "WidomGrad"]
+           "EwaldParams", "FrameworkBatch", "widom", "WidomResult", "B200Backend", "widom_grad", "WidomGrad",
+           "SystemState", "widom_chain", "widom_along_chain", "insertion_constant_term"]

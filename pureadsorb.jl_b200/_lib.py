@@ -42,9 +42,14 @@ class BatchDesc(ctypes.Structure):
                 ("framework_of", _p)]
 
 
+class ChainArgs(ctypes.Structure):
+    _fields_ = [("Sk", _p), ("const_term", _p), ("guest_offsets", _p), ("guest_sites", _p), ("k_offset", _i64)]
+
+
 class WidomArgs(ctypes.Structure):
     _fields_ = [("kT", _f64), ("ninsert", _i64), ("seed", _u64), ("nblocks", _i32), ("run", _i32),
-                ("reject", _i32), ("rho2", _p), ("reach0", _p), ("segment_begin", _i64), ("segment_end", _i64)]
+                ("reject", _i32), ("rho2", _p), ("reach0", _p), ("segment_begin", _i64), ("segment_end", _i64),
+                ("chain", ctypes.POINTER(ChainArgs))]
 
 
 class BlockSums(ctypes.Structure):

@@ -62,6 +62,10 @@ struct pa_context {
     DevMem abin, aslot, asorted, acount, afine_start, abin_start, atile_start;
     // adjoint workspace
     DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
+    // insertion into a loaded configuration: per-call tables and the guest-guest term
+    DevMem chain_kS2, chain_const, chain_goff, chain_gsites, chain_gtype, chain_cells, dUg;
+    std::vector<double> up_chain_kS2, up_chain_const, up_chain_gsites, up_chain_cells;
+    std::vector<int32_t> up_chain_goff, up_chain_gtype;
     // launch choices, the replayable graph of the last call's device sequence and its key
     pa_tuning tuning{0.0, 0, 0};
     cudaGraphExec_t gexec = nullptr;
@@ -102,6 +106,8 @@ struct pa_batch {
     // k-vector (inside the arena), and the (site, type) pair parameters of the desc
     const double* frac64 = nullptr;
     const double* kpref2 = nullptr;
+    std::vector<double> kpref2_h;  // host copy of 2 kpref per k-vector
+    std::vector<double> cells_h, invcells_h;  // FP64 cells (9 per framework, column-major)
     std::vector<double> site_sigma, site_eps;
     std::vector<int32_t> guest_types;  // 0-based compact type of each guest site
     std::vector<double> guest_q;       // guest site charges
@@ -483,6 +489,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     PA_CUDA(ctx, cudaMemcpyAsync(B->arena, ctx->h_stage, pk.n, cudaMemcpyHostToDevice, st));
     char* base = static_cast<char*>(B->arena);
     B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
+    B->kpref2_h = kpref2;
+    B->cells_h.assign(desc->cells, desc->cells + 9 * nfw);
+    B->invcells_h.assign(desc->invcells, desc->invcells + 9 * nfw);
     B->q64 = reinterpret_cast<const double*>(base + t_q64);
     B->types0 = reinterpret_cast<const int32_t*>(base + o.types);
     if (lists) B->frac64 = reinterpret_cast<const double*>(base + t_frac);
@@ -566,15 +575,15 @@ cudaError_t prepare_energy(const pa_batch* B) {
 }
 
 template <int NS>
-cudaError_t launch_energy(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms, int32_t ctas,
-                          cudaStream_t st) {
+cudaError_t launch_energy(const pa_batch* B, const pa::DevBatch<float>& v32, const pa::CallArgs& ca, const pa::Work& w,
+                          int32_t num_sms, int32_t ctas, cudaStream_t st) {
     if (B->precision == PA_PRECISION_F32) {
         const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
         const int32_t per = (ctas >= 1 && ctas <= PA_CTAS_PER_SM32) ? ctas : PA_CTAS_PER_SM32;
-        if (B->d32.rl2 == B->d32.re2)
-            pa::k_energy32<NS, true><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+        if (v32.rl2 == v32.re2)
+            pa::k_energy32<NS, true><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(v32, ca, w);
         else
-            pa::k_energy32<NS, false><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(B->d32, ca, w);
+            pa::k_energy32<NS, false><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(v32, ca, w);
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
@@ -596,10 +605,10 @@ cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Wor
 
 // The FP32 path's reciprocal term (charged guests) and the per-insertion sum of the site terms.
 template <int NS>
-cudaError_t launch_recip_combine(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, int32_t num_sms,
-                                 cudaStream_t st) {
-    if (B->d32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(B->d32, ca, w);
-    pa::k_combine<NS><<<unsigned((ca.n_act + 255) / 256), 256, 0, st>>>(B->d32, ca, w);
+cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallArgs& ca, const pa::Work& w,
+                                 int32_t num_sms, cudaStream_t st) {
+    if (v32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+    pa::k_combine<NS><<<unsigned((ca.n_act + 255) / 256), 256, 0, st>>>(v32, ca, w);
     return cudaGetLastError();
 }
 
@@ -859,6 +868,23 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     if (!(std::isfinite(args->kT) && args->kT != 0)) return fail(ctx, PA_ERR_ARG, "kT must be finite and nonzero");
     if (args->reject && (!args->rho2 || !args->reach0)) return fail(ctx, PA_ERR_ARG, "reject needs rho2 and reach0");
     const int nsys = B->nsys, N = B->nguest, nt = B->ntypes;
+    const pa_chain_args* chain = args->chain;
+    if (chain) {
+        if (B->precision != PA_PRECISION_F32)
+            return fail(ctx, PA_ERR_ARG, "insertion into a loaded configuration needs a batch uploaded for PA_PRECISION_F32");
+        if (args->reject) return fail(ctx, PA_ERR_ARG, "insertion into a loaded configuration is single-phase (reject = 0)");
+        bool own = B->nfw == nsys;
+        for (int s = 0; own && s < nsys; ++s) own = B->framework_of[s] == s + 1;
+        if (!own) return fail(ctx, PA_ERR_ARG, "insertion into a loaded configuration needs one framework per system");
+        if (!chain->const_term || !chain->guest_offsets || (B->nk > 0 && !chain->Sk))
+            return fail(ctx, PA_ERR_ARG, "null chain table");
+        if (chain->k_offset < 0) return fail(ctx, PA_ERR_ARG, "k_offset must be >= 0");
+        if (chain->guest_offsets[0] != 0) return fail(ctx, PA_ERR_ARG, "guest_offsets[0] must be 0");
+        for (int s = 0; s < nsys; ++s)
+            if (chain->guest_offsets[s + 1] < chain->guest_offsets[s])
+                return fail(ctx, PA_ERR_ARG, "guest_offsets must be nondecreasing");
+        if (chain->guest_offsets[nsys] > 0 && !chain->guest_sites) return fail(ctx, PA_ERR_ARG, "null guest_sites");
+    }
     std::vector<int64_t> ns = system_counts(ninsert, nsys, run);
     for (int s = 0; s < nsys; ++s)
         if (ns[s] < nblocks)
@@ -930,10 +956,47 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     }
     {
         const uint64_t seed = args->seed;
-        std::vector<double> sv(2);
+        const int64_t koff = chain ? chain->k_offset : 0;
+        std::vector<double> sv(3);
         std::memcpy(&sv[0], &seed, sizeof(double));
         sv[1] = args->kT;
+        std::memcpy(&sv[2], &koff, sizeof(double));
         PA_CUDA(ctx, upload_cached(ctx->scal, ctx->up_scal, sv, st));
+    }
+    // a loaded configuration: the systems' running S(k) (as 2 kpref S, the form of the batch's own
+    // table) and pose-independent terms replace the batch's, plus the live guests' sites
+    pa::DevBatch<float> v32;  // byte copy (padding included: the bytes key the CUDA graph)
+    std::memcpy(&v32, &B->d32, sizeof(v32));
+    pa::ChainArgs cargs{};
+    int64_t ng = 0;
+    if (chain) {
+        ng = chain->guest_offsets[nsys];
+        std::vector<double> ks2(std::max<int64_t>(2, 2 * B->nk), 0.0);
+        for (int64_t i = 0; i < B->nk; ++i) {
+            ks2[2 * i] = B->kpref2_h[i] * chain->Sk[2 * i];
+            ks2[2 * i + 1] = B->kpref2_h[i] * chain->Sk[2 * i + 1];
+        }
+        std::vector<double> ct(chain->const_term, chain->const_term + nsys);
+        std::vector<int32_t> go(chain->guest_offsets, chain->guest_offsets + nsys + 1);
+        std::vector<double> gs(std::max<int64_t>(3, 3 * ng * N), 0.0);
+        if (ng > 0) std::copy(chain->guest_sites, chain->guest_sites + 3 * ng * N, gs.begin());
+        std::vector<int32_t> gt(B->guest_types.begin(), B->guest_types.end());
+        std::vector<double> cl(B->cells_h);
+        cl.insert(cl.end(), B->invcells_h.begin(), B->invcells_h.end());
+        PA_CUDA(ctx, upload_cached(ctx->chain_kS2, ctx->up_chain_kS2, ks2, st));
+        PA_CUDA(ctx, upload_cached(ctx->chain_const, ctx->up_chain_const, ct, st));
+        PA_CUDA(ctx, upload_cached(ctx->chain_goff, ctx->up_chain_goff, go, st));
+        PA_CUDA(ctx, upload_cached(ctx->chain_gsites, ctx->up_chain_gsites, gs, st));
+        PA_CUDA(ctx, upload_cached(ctx->chain_gtype, ctx->up_chain_gtype, gt, st));
+        PA_CUDA(ctx, upload_cached(ctx->chain_cells, ctx->up_chain_cells, cl, st));
+        PA_CUDA(ctx, ctx->dUg.ensure(sizeof(double) * n_act));
+        v32.kS2 = ctx->chain_kS2.as<double>();
+        v32.const_offset = ctx->chain_const.as<double>();
+        cargs.gsites = ctx->chain_gsites.as<double>();
+        cargs.goff = ctx->chain_goff.as<int32_t>();
+        cargs.gtype = ctx->chain_gtype.as<int32_t>();
+        cargs.cells = ctx->chain_cells.as<double>();
+        cargs.invcells = ctx->chain_cells.as<double>() + 9 * B->nfw;
     }
     // pinned staging for the segment sums and counters (a graph copies into it)
     if (ctx->h_seg_cap < size_t(3 * nseg)) {
@@ -950,6 +1013,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     w.dU = ctx->dU.as<double>(); w.bin_count = ctx->bin_count.as<int32_t>(); w.fine_start = ctx->fine_start.as<int32_t>(); w.bin_start = ctx->bin_start.as<int32_t>();
     w.tile_start = ctx->tile_start.as<int32_t>(); w.counters = ctx->counters.as<int32_t>();
     w.seg_out = ctx->seg_out.as<double>(); w.seg_rng = ctx->seg_rng.as<int64_t>();
+    if (chain && ng > 0) w.dUg = ctx->dUg.as<double>();
     pa::Work wi = w;  // the item-level view: its own sort arrays and counters
     if (f32) {
         w.item_bin = ctx->item_bin.as<int32_t>(); w.item_slot = ctx->item_slot.as<int32_t>();
@@ -971,6 +1035,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     ca.i_lo = i_lo; ca.n_act = n_act; ca.sys_off = ctx->sys_off.as<int64_t>(); ca.seed = args->seed;
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
     ca.seed_dev = ctx->scal.as<uint64_t>(); ca.kT_dev = ctx->scal.as<double>() + 1;
+    ca.k_offset = chain ? chain->k_offset : 0; ca.koff_dev = reinterpret_cast<const int64_t*>(ctx->scal.as<double>() + 2);
     {
         cudaError_t e = cudaSuccess;
         PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
@@ -990,7 +1055,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             const unsigned gr = unsigned((n_act + 255) / 256);
             {
                 Timer tm(ctx, 0);
-                PA_DISPATCH_NS(N, (pa::k_draw32<NSV><<<gr, 256, 0, st>>>(B->d32, ca, w, wa)));
+                PA_DISPATCH_NS(N, (pa::k_draw32<NSV><<<gr, 256, 0, st>>>(v32, ca, w, wa)));
                 tm.stop(1);
             }
             {
@@ -1001,7 +1066,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             }
             {
                 Timer tm(ctx, 0);
-                PA_DISPATCH_NS(N, (pa::k_phase0_32<NSV><<<gr, 256, 0, st>>>(B->d32, ca, w, wa.sorted, ctx->rho2.as<float>(),
+                PA_DISPATCH_NS(N, (pa::k_phase0_32<NSV><<<gr, 256, 0, st>>>(v32, ca, w, wa.sorted, ctx->rho2.as<float>(),
                                                                                ctx->reach0.as<int32_t>())));
                 tm.stop(1);
             }
@@ -1027,15 +1092,22 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         {
             Timer tm(ctx, 2);
             cudaError_t e = cudaSuccess;
-            PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, f32 ? wi : w, ctx->num_sms, ctas, st)));
+            PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, v32, ca, f32 ? wi : w, ctx->num_sms, ctas, st)));
             tm.stop(1);
             if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
+        }
+        if (chain && ng > 0) {
+            Timer tm(ctx, 2);
+            const unsigned gg = unsigned(std::min<int64_t>((n_act + 7) / 8, int64_t(ctx->num_sms) * 16));
+            PA_DISPATCH_NS(N, (pa::k_guest32<NSV><<<gg, 256, 0, st>>>(v32, ca, w, cargs)));
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
         }
         if (f32) {
             Timer tm(ctx, 6);
             cudaError_t e = cudaSuccess;
-            PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B, ca, w, ctx->num_sms, st)));
-            tm.stop(B->d32.has_charge ? 2 : 1);
+            PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(v32, ca, w, ctx->num_sms, st)));
+            tm.stop(v32.has_charge ? 2 : 1);
             if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("reciprocal kernel launch: ") + cudaGetErrorString(e));
         }
         {
@@ -1053,25 +1125,28 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         // arguments (the batch's device view byte for byte, so a re-upload of the same batch into
         // the same pooled addresses replays) and the workspace addresses
         struct GraphKey {
-            const void* ptrs[36];
+            const void* ptrs[43];
             int64_t i_lo, n_act, nseg, nfine;
-            int32_t nbins, N, f32, reject, ctas, pad;
+            int32_t nbins, N, f32, reject, ctas, guests;
         } key;
         std::memset(&key, 0, sizeof(key));
-        const void* ps[36] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
+        const void* ps[43] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
                               ctx->bin_count.p, ctx->fine_start.p, ctx->bin_start.p, ctx->tile_start.p, ctx->counters.p,
                               ctx->seg_out.p, ctx->seg_rng.p, ctx->sys_off.p, ctx->rho2.p, ctx->reach0.p, ctx->scal.p,
                               ctx->h_seg, ctx->h_cnt, ctx->item_bin.p, ctx->item_slot.p, ctx->item_sorted.p,
                               ctx->item_count.p, ctx->item_fine_start.p, ctx->item_bin_start.p, ctx->item_tile_start.p,
                               ctx->dUs.p, ctx->abin.p, ctx->aslot.p, ctx->asorted.p, ctx->acount.p, ctx->afine_start.p,
-                              ctx->abin_start.p, ctx->atile_start.p, ctx->dUr.p};
+                              ctx->abin_start.p, ctx->atile_start.p, ctx->dUr.p, ctx->dUg.p, ctx->chain_kS2.p,
+                              ctx->chain_const.p, ctx->chain_goff.p, ctx->chain_gsites.p, ctx->chain_gtype.p,
+                              ctx->chain_cells.p};
         std::memcpy(key.ptrs, ps, sizeof(ps));
         key.i_lo = i_lo; key.n_act = n_act; key.nseg = nseg; key.nfine = nfine;
         key.nbins = B->nbins; key.N = N; key.f32 = f32 ? 1 : 0; key.reject = ca.reject; key.ctas = ctas;
+        key.guests = (chain && ng > 0) ? 1 : 0;
         const unsigned char* kp = reinterpret_cast<const unsigned char*>(&key);
         std::vector<unsigned char> kb(kp, kp + sizeof(key));
-        const unsigned char* vp = f32 ? reinterpret_cast<const unsigned char*>(&B->d32) : reinterpret_cast<const unsigned char*>(&B->d64);
-        kb.insert(kb.end(), vp, vp + (f32 ? sizeof(B->d32) : sizeof(B->d64)));
+        const unsigned char* vp = f32 ? reinterpret_cast<const unsigned char*>(&v32) : reinterpret_cast<const unsigned char*>(&B->d64);
+        kb.insert(kb.end(), vp, vp + (f32 ? sizeof(v32) : sizeof(B->d64)));
         const bool have = ctx->gexec && kb == ctx->gkey;
         if (!have && kb != ctx->last_key) {
             // a shape seen for the first time runs directly: capturing pays off from its
@@ -1148,6 +1223,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
 pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args* args, pa_block_sums* sums,
                         pa_grad_sums* grad, pa_insertion_out* per) {
     if (!ctx || !B || !args || !sums || !grad) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (args->chain) return fail(ctx, PA_ERR_ARG, "pa_widom_grad does not take a loaded configuration");
     if (B->precision != PA_PRECISION_F32) return fail(ctx, PA_ERR_ARG, "pa_widom_grad needs a batch uploaded for PA_PRECISION_F32");
     if (!grad->xmax || !grad->sum_w || !grad->d_epsilon || !grad->d_sigma || !grad->d_charge)
         return fail(ctx, PA_ERR_ARG, "null adjoint output array");
@@ -1406,6 +1482,7 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     if (!sums->lse_max || !sums->sum_w || !sums->sum_uw || !sums->count) return fail(ctx, PA_ERR_ARG, "null block-sum array");
     if (per && (per->flags || per->poses))
         return fail(ctx, PA_ERR_ARG, "pa_widom_static returns per-insertion dU only (flags and poses need host staging)");
+    if (args->chain) return fail(ctx, PA_ERR_ARG, "pa_widom_static does not take a loaded configuration");
     const int64_t ninsert = args->ninsert, nblocks = args->nblocks, run = args->run;
     if (ninsert < 1 || nblocks < 1 || run < 1) return fail(ctx, PA_ERR_ARG, "ninsert, nblocks and run must be >= 1");
     if (!(std::isfinite(args->kT) && args->kT != 0)) return fail(ctx, PA_ERR_ARG, "kT must be finite and nonzero");
@@ -1522,8 +1599,8 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     {
         cudaError_t e = cudaSuccess;
         PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
-        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
-        if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B, ca, w, ctx->num_sms, st))); }
+        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, B->d32, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
+        if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B->d32, ca, w, ctx->num_sms, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
     }
     pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT, nullptr);

@@ -75,7 +75,13 @@ struct CallArgs {
     // launch sequence captured in a CUDA graph replays for any seed and temperature
     const uint64_t* seed_dev;
     const double* kT_dev;
+    // added to every insertion's per-system index k (the insertions of one cycle along a chain
+    // follow the previous cycles'); koff_dev, when set, is read instead (graph replays)
+    int64_t k_offset;
+    const int64_t* koff_dev;
 };
+
+__device__ __forceinline__ int64_t k_shift(const CallArgs& ca) { return ca.koff_dev ? *ca.koff_dev : ca.k_offset; }
 
 // Per-call device workspace.
 struct Work {
@@ -101,6 +107,7 @@ struct Work {
     int32_t* item_count;  // nbins*nsub+1: items per sub-bin
     double* dUs;          // n_act*NS: real-space energy of each item's site
     double* dUr;          // n_act: KE times the reciprocal cross term
+    double* dUg;          // n_act: guest-guest real-space term (insertion along a chain), else NULL
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -274,7 +281,7 @@ __global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Wor
     const int64_t k = i - ca.sys_off[s] + 1;
     const int32_t fw = b.framework_of[s];
     F rp[3], qt[4];
-    draw_pose<F>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    draw_pose<F>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k + k_shift(ca)), rp, qt);
     if (sizeof(F) == 4) {
         w.pose_a[t] = make_float4(float(rp[0]), float(rp[1]), float(rp[2]), 0.0f);
         w.pose_b[t] = make_float4(float(qt[0]), float(qt[1]), float(qt[2]), float(qt[3]));
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(256) k_draw32(DevBatch<float> b, CallArgs ca, 
     const int64_t k = i - ca.sys_off[s] + 1;
     const int32_t fw = b.framework_of[s];
     float rp[3], qt[4];
-    draw_pose<float>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k), rp, qt);
+    draw_pose<float>(ca.seed_dev ? *ca.seed_dev : ca.seed, uint64_t(s + 1), uint64_t(k + k_shift(ca)), rp, qt);
     w.pose_a[t] = make_float4(rp[0], rp[1], rp[2], 0.0f);
     w.pose_b[t] = make_float4(qt[0], qt[1], qt[2], qt[3]);
     const int32_t fine = sub_bin_of(b, fw, rp[0], rp[1], rp[2]);
@@ -331,8 +338,8 @@ __global__ void __launch_bounds__(256, 4) k_phase0_32(DevBatch<float> b, CallArg
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_combine (FP32 path): ΔU = Σ_sites (real-space site sums) + KE E_lr + constant offset, in a
-// fixed order; rejected insertions keep +inf.
+// k_combine (FP32 path): ΔU = Σ_sites (real-space site sums) + KE E_lr (+ the guest-guest term
+// along a chain) + constant offset, in a fixed order; rejected insertions keep +inf.
 // ---------------------------------------------------------------------------------------------
 template <int NS>
 __global__ void __launch_bounds__(256) k_combine(DevBatch<float> b, CallArgs ca, Work w) {
@@ -344,6 +351,7 @@ __global__ void __launch_bounds__(256) k_combine(DevBatch<float> b, CallArgs ca,
 #pragma unroll
     for (int a = 1; a < NS; ++a) e += w.dUs[t * NS + a];
     if (b.has_charge) e += w.dUr[t];
+    if (w.dUg) e += w.dUg[t];
     w.dU[t] = e + b.const_offset[fw];
 }
 
@@ -511,6 +519,7 @@ __device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
 
 #include "pa_energy32.cuh"
 #include "pa_grad32.cuh"
+#include "pa_chain32.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // k_energy64: the plain FP64 form of the reference algorithm (src/energy.jl:42-82): for every
