@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-fit", action="store_true")
+    p.add_argument("--no-chain", action="store_true")
     p.add_argument("--no-tune", action="store_true", help="default bin width and grid (e.g. for profiling)")
     return p.parse_args()
 
@@ -154,6 +155,83 @@ def cpu_baseline_port(pa, orc, batch, guest, ninsert_full, target_s=12.0, nthrea
         if dt > 0.25 * target_s or n >= ninsert_full:
             return n / dt, n, (nthreads or os.cpu_count())
         n = int(min(ninsert_full, n * max(2.0, 0.5 * target_s / max(dt, 1e-3))))
+
+
+def chain_workload(pa, orc, backend, torch, stream, flush, no_cpu=False):
+    """Widom along an NVT chain on the CO2 framework: its full k table (fullk, every k-vector of
+    the supercell), two systems sharing the framework at 10 and 40 CO2 guests (placed clear of the
+    host's hard core), 2^18 insertions per system per cycle, no rejection, as widom_chain_kernel!
+    computes them; CUDA events around each cycle's call (graph-replayed, the cycle index moving the
+    pose stream on), per-kernel times from one timed call, and the FP64 oracle's chain energy on the
+    host cores over a sample of the same insertions."""
+    ctx = backend.ctx
+    fws, ff, guest, ewald, prm = pa.synthetic.co2(T=np.float32)
+    t0 = time.perf_counter()
+    b = pa.FrameworkBatch(fws * 2, ff, guest, ewald, fullk=True)
+    st = pa.SystemState.placed(b, guest, [10, 40], T=prm["T"], seed=1001)
+    build_s = time.perf_counter() - t0
+    nper, T, seed = 2**18, prm["T"], prm["seed"]
+    ctx.set_tuning(bin_width=3.5, ctas_per_sm=8, use_graphs=True)
+
+    def cycle(c, **kw):
+        return pa.widom_chain(b, st, guest, ff, T=T, n_widom_per_cycle=nper, seed=seed, cycle=c, backend=backend, **kw)
+
+    for c in range(2):
+        cycle(c)
+    ms = []
+    for c in range(2, 7):
+        flush.zero_()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cycle(c)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(e))
+    ms_cycle = float(np.median(ms))
+    ctx.set_timing(True)
+    k0, _ = ctx.kernel_times()
+    cycle(7)
+    torch.cuda.synchronize()
+    k1, _ = ctx.kernel_times()
+    ctx.set_timing(False)
+    kd = k1 - k0
+    out = {"workload": "chain_co2_5832_atoms_fullk_2_systems", "systems": 2, "guests": [10, 40],
+           "k_vectors_per_system": int(len(b.ks)), "ninsert_per_cycle": 2 * nper, "ms_per_cycle": ms_cycle,
+           "value": 2 * nper / (ms_cycle / 1e3), "unit": "insertions/s",
+           "kernel_ms": {"poses": float(kd[0]), "scan_scatter": float(kd[1]), "energy": float(kd[2]),
+                         "guest_guest": float(kd[7]), "reciprocal_combine": float(kd[6]), "segment_reduce": float(kd[3])},
+           "build_s": build_s}
+    if not no_cpu:
+        # the oracle's FP64 chain energy at the device's poses of a sample cycle, OpenMP on the host
+        ns = 4096
+        ins = {}
+        pa.widom_chain(b, st, guest, ff, T=T, n_widom_per_cycle=ns, seed=seed, cycle=0, backend=backend,
+                       insertions=ins)
+        sb = pa.chain.system_batch(b)
+        vb = type("View", (), {})()
+        for k in ("positions", "types", "charges", "atom_offsets", "cells", "invcells", "volumes", "alphas", "ks",
+                  "kprefactor", "k_offsets", "constant_offset", "ncells", "cell_offsets", "cellgrid_offsets", "sigma",
+                  "epsilon", "guest_types", "framework_of"):
+            setattr(vb, k, getattr(sb, k))
+        vb.Shost = st.Sk
+        v, keep = orc.view(vb, b.guest_sites_orig, b.guest_charges_orig, b.cutoff, b.ewald_cutoff)
+        kT = float(b.T(pa.KB * T))
+        t0 = time.perf_counter()
+        dln = []
+        for s in range(2):
+            sl = slice(s * ns, (s + 1) * ns)
+            ref = orc.chain_energy(v, s, ins["poses"][sl, :3] @ sb.cells[s].T, ins["poses"][sl, 3:],
+                                   st.live_sites(guest, s))
+            ref += pa.insertion_constant_term(ff, b, guest, s, st.nguests(s))
+            with np.errstate(over="ignore"):
+                dln.append(abs(math.log(np.sum(np.exp(-ins["dU"][sl] / kT))) - math.log(np.sum(np.exp(-ref / kT)))))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 2 * ns / dt, "unit": "insertions/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"{2 * ns} insertions of the workload (FP64 oracle chain energy, OpenMP)"}
+        out["sample_max_dlnW"] = float(max(dln))
+    b.drop_device()
+    pa.chain.system_batch(b).drop_device()
+    return out
 
 
 def batched_workload(pa, backend, torch, stream, flush):
@@ -458,6 +536,8 @@ def main():
                    "note": "widom_grad: forward pass + adjoint pass + host chain rule, CUDA events around the call"}
 
         batched = None if args.no_batched or world > 1 else batched_workload(pa, backend, torch, stream, flush)
+        chain = None if args.no_chain or world > 1 else chain_workload(pa, orc, backend, torch, stream, flush,
+                                                                       no_cpu=args.no_cpu)
         fitting = None if args.no_fit or world > 1 else fitting_workload(pa, backend)
 
         cpu = None
@@ -488,6 +568,7 @@ def main():
                 "fp64_plain": fp64,
                 "adjoint": adj,
                 "batched": batched,
+                "chain": chain,
                 "fitting": fitting,
                 "e2e": {"value": e2e_value, "unit": "insertions/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},

@@ -58,8 +58,8 @@ pa_status pa_context_set_timing(pa_context* ctx, int32_t enable);
 /* Total device milliseconds and launch counts per kernel class since timing was enabled.
  * Classes: 0 pose+phase-0, 1 scan/scatter, 2 energy (real space), 3 reduction, 4 neighbour-list
  * build, 5 adjoint (selection, recomputation, reciprocal charge term), 6 FP32 reciprocal term and
- * per-insertion sum. */
-pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*7*/, int64_t* launches /*7*/);
+ * per-insertion sum, 7 guest-guest term of an insertion into a loaded configuration. */
+pa_status pa_context_kernel_times(pa_context* ctx, double* ms /*8*/, int64_t* launches /*8*/);
 
 /* Layout and launch choices of a context (no counterpart in the reference), set by the
  * autotuner or by hand. bin_width: edge in Å of the FP32 path's spatial bins, applied to batches

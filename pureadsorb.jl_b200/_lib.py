@@ -200,8 +200,8 @@ class Context:
         return t
 
     def kernel_times(self):
-        ms = np.zeros(7)
-        n = np.zeros(7, dtype=np.int64)
+        ms = np.zeros(8)
+        n = np.zeros(8, dtype=np.int64)
         self.check(lib().pa_context_kernel_times(self.handle, ptr(ms), ptr(n)), "pa_context_kernel_times")
         return ms, n
 

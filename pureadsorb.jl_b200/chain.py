@@ -94,14 +94,27 @@ class SystemState:
 
     def live_sites(self, guest, s):
         """Absolute site positions of system s's live guests, (nguests, N, 3) (guest_sites_at,
-        src/guest.jl:78)."""
+        src/guest.jl:78): refpoint + v + 2 u x (u x v + w v) per site (src/energy.jl:13-16)."""
         j0 = int(self.guest_offsets[s])
         n = int(self.occupancy[s])
-        out = np.zeros((n, len(guest.sites), 3))
-        for j in range(n):
-            for a, site in enumerate(guest.sites):
-                out[j, a] = self.refpoints[j0 + j] + _rotate(self.orientations[j0 + j], site)
-        return out
+        q = self.orientations[j0:j0 + n]
+        u, w = q[:, None, :3], q[:, None, 3:4]
+        v = np.asarray(guest.sites, dtype=np.float64)[None, :, :]
+        c = np.cross(u, v) + w * v
+        return self.refpoints[j0:j0 + n, None, :] + v + 2 * np.cross(u, c)
+
+    def chain_inputs(self, guest):
+        """The per-call tables of a device call (cached: a SystemState is not modified after
+        construction): S(k) as (re, im) pairs, live-guest offsets and their site positions."""
+        cached = self.__dict__.get("_chain_inputs")
+        if cached is not None:
+            return cached
+        Sk = np.ascontiguousarray(np.stack([self.Sk.real, self.Sk.imag], axis=1).reshape(-1))
+        live = [self.live_sites(guest, s) for s in range(self.nsys)]
+        goff = np.concatenate([[0], np.cumsum([len(x) for x in live])]).astype(np.int32)
+        sites = np.ascontiguousarray(np.concatenate([x.reshape(-1) for x in live]) if goff[-1] else np.zeros(3))
+        self._chain_inputs = (Sk, goff, sites)
+        return self._chain_inputs
 
     @classmethod
     def placed(cls, batch, guest, ncounts, *, T, seed=0, capacities=None, max_draws=100_000):
@@ -265,10 +278,7 @@ def widom_chain(batch, state, guest, ff, *, T, n_widom_per_cycle, seed=0, cycle=
     ctx = backend.ctx
     dev = sb.device(ctx)
     const = np.array([insertion_constant_term(ff, batch, guest, s, state.nguests(s)) for s in range(nsys)])
-    Sk = np.ascontiguousarray(np.stack([state.Sk.real, state.Sk.imag], axis=1).reshape(-1))
-    live = [state.live_sites(guest, s) for s in range(nsys)]
-    goff = np.concatenate([[0], np.cumsum([len(x) for x in live])]).astype(np.int32)
-    sites = np.ascontiguousarray(np.concatenate([x.reshape(-1) for x in live]) if goff[-1] else np.zeros(3))
+    Sk, goff, sites = state.chain_inputs(guest)
     chain = _lib.ChainArgs(_lib.ptr(Sk) if Sk.size else None, _lib.ptr(const), _lib.ptr(goff), _lib.ptr(sites),
                            int(cycle) * nper)
     n = nsys * nper

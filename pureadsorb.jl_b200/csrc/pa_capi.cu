@@ -21,7 +21,8 @@ static_assert(PA_SEGMENT_SIZE == PA_SEGMENT, "segment size mismatch");
 
 namespace {
 
-constexpr int NCLASS = 7;  // kernel classes: pose, scan/scatter, energy, reduce, lists, adjoint, reciprocal+combine
+constexpr int NCLASS = 8;  // kernel classes: pose, scan/scatter, energy, reduce, lists, adjoint, reciprocal+combine,
+                           // guest-guest
 constexpr double LIST_PAD = 32;
 constexpr double DEFAULT_BIN_WIDTH = 3.0;  // Angstrom, FP32 path spatial bins
 constexpr double WAIT_LIMIT_S = 600.0;      // host-side bound on one call's device work
@@ -1097,7 +1098,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
         }
         if (chain && ng > 0) {
-            Timer tm(ctx, 2);
+            Timer tm(ctx, 7);
             const unsigned gg = unsigned(std::min<int64_t>((n_act + 7) / 8, int64_t(ctx->num_sms) * 16));
             PA_DISPATCH_NS(N, (pa::k_guest32<NSV><<<gg, 256, 0, st>>>(v32, ca, w, cargs)));
             tm.stop(1);

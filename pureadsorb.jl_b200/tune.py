@@ -33,7 +33,7 @@ def _device_ms(ctx, call, repeats):
         call()
         ms, n = ctx.kernel_times()
         ctx.set_timing(False)
-        times.append(float(np.sum(ms[:4]) + ms[6]))
+        times.append(float(np.sum(ms[:4]) + ms[6] + ms[7]))
     return float(np.median(times))
 
 

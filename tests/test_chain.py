@@ -128,8 +128,9 @@ def test_oracle_chain_energy_matches_total_energy_difference(pa, orc, setup, ng,
     for m in range(nposes):
         test = np.array([pos[m] + pa.batch._rotate(quat[m], x) for x in guest.sites])[None]
         dU_ref[m] = total_energy(pa, orc, b, ff, guest, 0, np.concatenate([sites, test]), precision) - E0
-    # single poses: within the self-term spread
-    assert np.max(np.abs(dU - dU_ref)[np.isfinite(dU_ref)]) <= 2.6 * b.self_term_halfrange[0] + 1e-9
+    # single poses: within the self-term spread (plus FP64 rounding of overlapping poses' large ΔU)
+    fin = np.isfinite(dU_ref)
+    assert np.all(np.abs(dU - dU_ref)[fin] <= 2.6 * b.self_term_halfrange[0] + 1e-9 + 1e-12 * np.abs(dU_ref[fin]))
     w, wr = np.exp(-dU / kT), np.exp(-dU_ref / kT)
     se = math.sqrt(np.var(w, ddof=1) / nposes + np.var(wr, ddof=1) / nposes)
     assert abs(w.mean() - wr.mean()) <= 5 * se
