@@ -95,7 +95,7 @@ struct pa_batch {
     pa_context* ctx = nullptr;  // the uploading context; only compared, never dereferenced on free
     int32_t device = 0;
     int32_t precision = 0;
-    int32_t nsys = 0, nfw = 0, ntypes = 0, nguest = 0, nbins = 0;
+    int32_t nsys = 0, nfw = 0, ntypes = 0, nguest = 0, nbins = 0, runs_per_bin = 2;
     int64_t natoms = 0, nk = 0, list_entries = 0;
     std::vector<int32_t> framework_of, atom_offsets, k_offsets;
     // two stream-ordered allocations: the packed static tables, and the neighbour lists
@@ -295,7 +295,7 @@ pa_status wait_stream(pa_context* ctx) {
 struct Slots {
     size_t framework_of, cells, invcells, alphas, const_offset, atom_offsets, atoms, types, ncells, cell_offsets,
         cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, kpref2, sig2, eps4, bin_dims, bin_base, bin_fw;
-    size_t list_offsets, list_xyzq, list_type, list_atom;  // offsets inside the list allocation
+    size_t list_offsets, list_xyzq, list_type, list_atom, list_runs;  // offsets inside the list allocation
 };
 
 template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc, const Slots& o) {
@@ -336,6 +336,8 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     d.list_xyzq = l ? reinterpret_cast<const float4*>(l + o.list_xyzq) : nullptr;
     d.list_type = l ? reinterpret_cast<const int32_t*>(l + o.list_type) : nullptr;
     d.list_atom = l ? reinterpret_cast<const int32_t*>(l + o.list_atom) : nullptr;
+    d.list_runs = l ? reinterpret_cast<const int2*>(l + o.list_runs) : nullptr;
+    d.runs_per_bin = B->runs_per_bin;
 }
 
 template <typename F>
@@ -535,7 +537,18 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         o.list_xyzq = up256(sizeof(int32_t) * loff.size());
         o.list_type = up256(o.list_xyzq + sizeof(float4) * nent);
         o.list_atom = up256(o.list_type + sizeof(int32_t) * nent);
-        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_atom + sizeof(int32_t) * nent, st));
+        // type runs per bin: at most one per host type of the framework, one of padding, a sentinel
+        int32_t tmax = 0;
+        for (int fw = 0; fw < nfw; ++fw) {
+            std::vector<char> seen(nt, 0);
+            int32_t c = 0;
+            for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
+                if (!seen[types[j]]) { seen[types[j]] = 1; ++c; }
+            tmax = std::max(tmax, c);
+        }
+        B->runs_per_bin = tmax + 2;
+        o.list_runs = up256(o.list_atom + sizeof(int32_t) * nent);
+        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_runs + sizeof(int2) * size_t(std::max(1, B->nbins)) * B->runs_per_bin, st));
         PA_CUDA(ctx, cudaMemcpyAsync(B->lists, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st));
         char* lb = static_cast<char*>(B->lists);
         g.offsets = reinterpret_cast<const int32_t*>(lb + o.list_offsets);
@@ -545,7 +558,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         if (B->nbins > 0) {
             Timer tm(ctx, 4);
             pa::k_lists<true><<<B->nbins, 256, 0, st>>>(g);
-            tm.stop(1);
+            pa::k_runs<<<B->nbins, 32, 0, st>>>(g.offsets, g.type_out, reinterpret_cast<int2*>(lb + o.list_runs),
+                                                B->runs_per_bin);
+            tm.stop(2);
             PA_CUDA(ctx, cudaGetLastError());
         }
     }

@@ -69,7 +69,6 @@ __device__ __forceinline__ void bin_centre(const DevBatch<float>& b, int32_t fw,
 template <int NS, bool EQCUT>
 __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
-    __shared__ __align__(128) int32_t s_type[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[PA_WARPS32][2];
     __shared__ float4 s_site[NS];    // body-frame site offsets, and the site charge times KE
     extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
@@ -83,7 +82,6 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     const float* s_sig2 = s_lj;
     const float* s_eps4 = s_lj + NS * nt;
     float4(*xyzq)[PA_CHUNK32] = s_xyzq[wp];
-    int32_t(*typ)[PA_CHUNK32] = s_type[wp];
     uint64_t* bar = s_bar[wp];
     uint32_t gchunk = 0;  // chunks this warp has consumed (selects stage and parity)
     const bool charged = b.has_charge != 0;
@@ -98,9 +96,8 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                 const uint32_t st = (gchunk + c) & 1;
                 const int32_t e0 = l0 + c * PA_CHUNK32, n = min(PA_CHUNK32, l1 - e0);
                 fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&bar[st], uint32_t(n) * 20u);
+                mbar_arrive_expect_tx(&bar[st], uint32_t(n) * 16u);
                 bulk_g2s(xyzq[st], b.list_xyzq + e0, uint32_t(n) * 16u, &bar[st]);
-                bulk_g2s(typ[st], b.list_type + e0, uint32_t(n) * 4u, &bar[st]);
             }
         }
         const bool active = lo + lane < hi;
@@ -136,9 +133,11 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
         float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
         // LJ parameters of the current host type for this lane's site: list entries come in runs of
-        // one type, the same for every lane, so the reload is a uniform branch
-        int32_t cur = -1;
-        float sg = 0.f, ep = 0.f;
+        // one type (the bin's run table), the same for every lane, so the loop runs uniformly from
+        // one run boundary to the next and reloads them there
+        const int2* runs = b.list_runs + int64_t(bin) * b.runs_per_bin;
+        int32_t ri = 0, rnext = runs[1].x;
+        float sg = s_sig2[as * nt + runs[0].y], ep = s_eps4[as * nt + runs[0].y];
         // tmo_at: chunk whose copy did not arrive in time (-1: none); after it no copies are issued
         // and only the chunk already in flight is still waited for
         int32_t tmo_at = -1;
@@ -149,53 +148,58 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             if (late && tmo_at < 0) tmo_at = c;
             const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
             if (tmo_at < 0) {
+                const int32_t base = l0 + c * PA_CHUNK32;
+                int32_t j = 0;
+                for (;;) {
+                    const int32_t jend = min(n, rnext - base);
 #pragma unroll 4
-                for (int32_t j = 0; j < n; ++j) {
-                    const float4 at = xyzq[st][j];
-                    const int32_t ty = typ[st][j];
-                    if (ty != cur) {
-                        cur = ty;
-                        sg = s_sig2[as * nt + ty];
-                        ep = s_eps4[as * nt + ty];
-                    }
-                    const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
-                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    if (r2 < rc2) {
-                        float e = 0.f;
-                        if (charged) {
-                            // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
-                            float ri = rsqrt_ftz(r2);
-                            ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
-                            if (EQCUT || r2 < rl2) {
-                                const float x = sg * (ri * ri);
+                    for (; j < jend; ++j) {
+                        const float4 at = xyzq[st][j];
+                        const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (r2 < rc2) {
+                            float e = 0.f;
+                            if (charged) {
+                                // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
+                                float ri = rsqrt_ftz(r2);
+                                ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
+                                if (EQCUT || r2 < rl2) {
+                                    const float x = sg * (ri * ri);
+                                    const float x3 = x * x * x;
+                                    e = ep * (x3 * x3 - x3);
+                                }
+                                if (EQCUT || r2 < re2) {
+                                    const float z = alpha * (r2 * ri);
+                                    const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
+                                    const float cf[PA_NERFC32] = PA_ERFC32_INIT;
+                                    float p = cf[PA_NERFC32 - 1];
+#pragma unroll
+                                    for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
+                                    e = fmaf(qk * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
+                                }
+                            } else {
+                                const float x = sg * rcp_nr(r2);
                                 const float x3 = x * x * x;
                                 e = ep * (x3 * x3 - x3);
                             }
-                            if (EQCUT || r2 < re2) {
-                                const float z = alpha * (r2 * ri);
-                                const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
-                                const float cf[PA_NERFC32] = PA_ERFC32_INIT;
-                                float p = cf[PA_NERFC32 - 1];
-#pragma unroll
-                                for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
-                                e = fmaf(qk * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
-                            }
-                        } else {
-                            const float x = sg * rcp_nr(r2);
-                            const float x3 = x * x * x;
-                            e = ep * (x3 * x3 - x3);
+                            kahan_add(esum, ecmp, e);
                         }
-                        kahan_add(esum, ecmp, e);
                     }
+                    if (j >= n) break;
+                    // entry j starts the next type run
+                    ++ri;
+                    const int32_t ty = runs[ri].y;
+                    rnext = runs[ri + 1].x;
+                    sg = s_sig2[as * nt + ty];
+                    ep = s_eps4[as * nt + ty];
                 }
             }
             __syncwarp();  // the warp is done with stage st
             if (lane == 0 && tmo_at < 0 && c + 2 < nch) {
                 const int32_t e0 = l0 + (c + 2) * PA_CHUNK32, nn = min(PA_CHUNK32, l1 - e0);
                 fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&bar[st], uint32_t(nn) * 20u);
+                mbar_arrive_expect_tx(&bar[st], uint32_t(nn) * 16u);
                 bulk_g2s(xyzq[st], b.list_xyzq + e0, uint32_t(nn) * 16u, &bar[st]);
-                bulk_g2s(typ[st], b.list_type + e0, uint32_t(nn) * 4u, &bar[st]);
             }
         }
         gchunk += uint32_t(nch);

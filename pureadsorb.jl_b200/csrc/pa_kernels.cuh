@@ -62,6 +62,9 @@ struct DevBatch {
     const float4* list_xyzq;                      // imaged position relative to the bin centre, charge
     const int32_t* list_type;                     // 0-based type (padding entries: type 0, far away)
     const int32_t* list_atom;                     // stored-atom index of each entry
+    const int2* list_runs;                        // nbins*runs_per_bin: each bin's type runs (first entry,
+                                                  // type), then (end of the list, 0) up to runs_per_bin
+    int32_t runs_per_bin;
 };
 
 // Per-call arguments shared by the kernels.
@@ -714,6 +717,31 @@ struct ListGeom {
 // images inside that box (a margin far above FP32 rounding keeps every image the strict test
 // would keep); an ordered block scan of the per-thread counts then places its entries. Count and
 // fill passes make the same tests, so the fill writes exactly the counted entries.
+// The type runs of every bin's list (entries are in type-major order): one warp per bin, the run
+// starts found by ballot in entry order; the remaining slots (at least one) hold (end, 0).
+__global__ void __launch_bounds__(32) k_runs(const int32_t* offsets, const int32_t* type, int2* runs, int32_t rm) {
+    const int32_t bin = blockIdx.x, lane = threadIdx.x;
+    const int32_t l0 = offsets[bin], l1 = offsets[bin + 1];
+    int2* r = runs + int64_t(bin) * rm;
+    int32_t k = 0;
+    for (int32_t e0 = l0; e0 < l1; e0 += 32) {
+        const int32_t e = e0 + lane;
+        bool start = false;
+        int32_t t = 0;
+        if (e < l1) {
+            t = type[e];
+            start = e == l0 || type[e - 1] != t;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, start);
+        if (start) {
+            const int32_t idx = k + __popc(bal & ((1u << lane) - 1u));
+            if (idx < rm - 1) r[idx] = make_int2(e, t);
+        }
+        k += __popc(bal);
+    }
+    for (int32_t i = min(k, rm - 1) + lane; i < rm; i += 32) r[i] = make_int2(l1, 0);
+}
+
 #define LIST_ATOMS 4
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
