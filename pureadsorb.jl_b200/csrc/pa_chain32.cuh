@@ -13,8 +13,9 @@
 // lose about 1e-7 of the cell length; r^2 is then rounded once and the pair terms use k_energy32's
 // FP32 arithmetic.
 //
-// One warp per insertion, lanes over the system's live guests. Included by pa_kernels.cuh after
-// pa_energy32.cuh.
+// One warp per insertion, lanes over the (live guest, guest site) pairs of the system (a system
+// holds tens of guests, so lanes over guests alone would leave most of the warp idle). Included by
+// pa_kernels.cuh after pa_energy32.cuh.
 #pragma once
 
 struct ChainArgs {
@@ -66,10 +67,11 @@ __global__ void __launch_bounds__(256) k_guest32(DevBatch<float> b, CallArgs ca,
         }
         float esum = 0.f, ecmp = 0.f;
         bool hit = false;  // coincident sites: the pair energy diverges
-        for (int32_t j = j0 + lane; j < j1; j += 32) {
-#pragma unroll
-            for (int bb = 0; bb < NS; ++bb) {
-                const double* o = c.gsites + 3 * (int64_t(j) * NS + bb);
+        const int64_t p1 = int64_t(j1 - j0) * NS;
+        for (int64_t p = lane; p < p1; p += 32) {
+            {
+                const int32_t bb = int32_t(p % NS);
+                const double* o = c.gsites + 3 * (int64_t(j0) * NS + p);
                 const double ox = o[0], oy = o[1], oz = o[2];
                 const int32_t tb = c.gtype[bb];
                 const float qb = b.gq[bb];
