@@ -261,8 +261,9 @@ typedef struct pa_grad_sums {
     double* d_charge;    /* Σ_s natoms(framework_of[s]) out: Σ_i w_i ∂ΔU_i/∂q_j per stored
                             atom j of the system's framework (desc order), system-major          */
     double* s_guest;     /* optional, 2*Σ_s nk(framework_of[s]): Σ_i w_i S_g,i(k) (re, im)      */
-    double window;       /* in: selection window in units of kT (0: 50)                         */
-    int64_t recomputed;  /* out: insertions the adjoint pass recomputed                         */
+    double window;       /* in: the charge pass recomputes survivors within this many kT of the
+                            system's largest weight (0: 50); the ε and σ sums cover every survivor */
+    int64_t recomputed;  /* out: insertions the charge pass recomputed (0 with lj_only)          */
     int32_t lj_only;     /* in: nonzero skips the charge derivatives (d_charge and s_guest are
                             returned as zeros), for callers that only need ε and σ               */
 } pa_grad_sums;

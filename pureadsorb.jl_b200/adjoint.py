@@ -29,8 +29,10 @@ from .widom import _results, _widom, default_backend, lnkh_from_sums
 @dataclass
 class WidomGrad:
     """d ln K_H / dθ of one system. epsilon and sigma: per force-field type (ff.names order,
-    1/eV and 1/Å); charges: per atom of the system's framework in the framework's own atom order
-    (1/e), None when the charge derivatives were not asked for; recomputed: insertions the adjoint pass recomputed; sum_w and xmax: the weight sums."""
+    1/eV and 1/Å), from every survivor's LJ sums kept by the forward pass; charges: per atom of
+    the system's framework in the framework's own atom order (1/e), None when the charge
+    derivatives were not asked for; recomputed: insertions the charge pass recomputed (0 without
+    charges); sum_w and xmax: the weight sums."""
 
     epsilon: np.ndarray
     sigma: np.ndarray

@@ -63,6 +63,9 @@ struct pa_context {
     DevMem abin, aslot, asorted, acount, afine_start, abin_start, atile_start;
     // adjoint workspace
     DevMem heavy, g_w, g_lj, g_q, g_k, xmax, sys_aoff, sys_koff;
+    // the forward pass of pa_widom_grad also stores each item's LJ sums per type run
+    bool want_pq = false;
+    DevMem item_pq;
     // insertion into a loaded configuration: per-call tables and the guest-guest term
     DevMem chain_kS2, chain_const, chain_goff, chain_gsites, chain_gtype, chain_cells, dUg;
     std::vector<double> up_chain_kS2, up_chain_const, up_chain_gsites, up_chain_cells;
@@ -585,8 +588,10 @@ cudaError_t prepare_energy(const pa_batch* B) {
     if (B->precision != PA_PRECISION_F32) return cudaSuccess;
     const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
     if (dyn <= 48 * 1024) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
     return e;
 }
 
@@ -596,10 +601,14 @@ cudaError_t launch_energy(const pa_batch* B, const pa::DevBatch<float>& v32, con
     if (B->precision == PA_PRECISION_F32) {
         const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
         const int32_t per = (ctas >= 1 && ctas <= PA_CTAS_PER_SM32) ? ctas : PA_CTAS_PER_SM32;
-        if (v32.rl2 == v32.re2)
-            pa::k_energy32<NS, true><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(v32, ca, w);
-        else
-            pa::k_energy32<NS, false><<<num_sms * per, 32 * PA_WARPS32, dyn, st>>>(v32, ca, w);
+        const unsigned grid = unsigned(num_sms * per), block = 32 * PA_WARPS32;
+        if (v32.rl2 == v32.re2) {
+            if (w.item_pq) pa::k_energy32<NS, true, true><<<grid, block, dyn, st>>>(v32, ca, w);
+            else pa::k_energy32<NS, true, false><<<grid, block, dyn, st>>>(v32, ca, w);
+        } else {
+            if (w.item_pq) pa::k_energy32<NS, false, true><<<grid, block, dyn, st>>>(v32, ca, w);
+            else pa::k_energy32<NS, false, false><<<grid, block, dyn, st>>>(v32, ca, w);
+        }
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
     }
@@ -956,6 +965,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         PA_CUDA(ctx, ctx->afine_start.ensure(sizeof(int32_t) * (nfine + 1)));
         PA_CUDA(ctx, ctx->abin_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
         PA_CUDA(ctx, ctx->atile_start.ensure(sizeof(int32_t) * (B->nbins + 1)));
+        if (ctx->want_pq) PA_CUDA(ctx, ctx->item_pq.ensure(sizeof(float2) * size_t(nit) * size_t(B->runs_per_bin)));
     }
     PA_CUDA(ctx, ctx->seg_out.ensure(sizeof(double) * 3 * nseg));
     // per-call tables, uploaded only when they differ from the last call's
@@ -1039,6 +1049,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         wi.bin_count = w.item_count; wi.fine_start = ctx->item_fine_start.as<int32_t>();
         wi.bin_start = ctx->item_bin_start.as<int32_t>(); wi.tile_start = ctx->item_tile_start.as<int32_t>();
         wi.counters = ctx->counters.as<int32_t>() + 8;
+        if (ctx->want_pq) wi.item_pq = ctx->item_pq.as<float2>();
     }
     pa::Work wa = w;  // the all-insertion view (FP32 phase 0 in sub-bin order)
     if (f32) {
@@ -1141,12 +1152,12 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         // arguments (the batch's device view byte for byte, so a re-upload of the same batch into
         // the same pooled addresses replays) and the workspace addresses
         struct GraphKey {
-            const void* ptrs[43];
+            const void* ptrs[44];
             int64_t i_lo, n_act, nseg, nfine;
             int32_t nbins, N, f32, reject, ctas, guests;
         } key;
         std::memset(&key, 0, sizeof(key));
-        const void* ps[43] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
+        const void* ps[44] = {st, ctx->pose_a.p, ctx->pose_b.p, ctx->bin_of.p, ctx->slot.p, ctx->sorted.p, ctx->dU.p,
                               ctx->bin_count.p, ctx->fine_start.p, ctx->bin_start.p, ctx->tile_start.p, ctx->counters.p,
                               ctx->seg_out.p, ctx->seg_rng.p, ctx->sys_off.p, ctx->rho2.p, ctx->reach0.p, ctx->scal.p,
                               ctx->h_seg, ctx->h_cnt, ctx->item_bin.p, ctx->item_slot.p, ctx->item_sorted.p,
@@ -1154,7 +1165,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
                               ctx->dUs.p, ctx->abin.p, ctx->aslot.p, ctx->asorted.p, ctx->acount.p, ctx->afine_start.p,
                               ctx->abin_start.p, ctx->atile_start.p, ctx->dUr.p, ctx->dUg.p, ctx->chain_kS2.p,
                               ctx->chain_const.p, ctx->chain_goff.p, ctx->chain_gsites.p, ctx->chain_gtype.p,
-                              ctx->chain_cells.p};
+                              ctx->chain_cells.p, ctx->want_pq ? ctx->item_pq.p : nullptr};
         std::memcpy(key.ptrs, ps, sizeof(ps));
         key.i_lo = i_lo; key.n_act = n_act; key.nseg = nseg; key.nfine = nfine;
         key.nbins = B->nbins; key.N = N; key.f32 = f32 ? 1 : 0; key.reject = ca.reject; key.ctas = ctas;
@@ -1244,7 +1255,10 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
     if (!grad->xmax || !grad->sum_w || !grad->d_epsilon || !grad->d_sigma || !grad->d_charge)
         return fail(ctx, PA_ERR_ARG, "null adjoint output array");
     if (!(grad->window >= 0)) return fail(ctx, PA_ERR_ARG, "window must be >= 0");
+    // the forward pass also keeps each item's LJ sums per type run (k_energy32's PQ form)
+    ctx->want_pq = true;
     pa_status stt = pa_widom(ctx, B, args, sums, per);
+    ctx->want_pq = false;
     if (stt != PA_OK) return stt;
     const int nsys = B->nsys, N = B->nguest, nt = B->ntypes;
     const int64_t nblocks = args->nblocks;
@@ -1308,14 +1322,25 @@ pa_status pa_widom_grad(pa_context* ctx, const pa_batch* B, const pa_widom_args*
     g.g_w = ctx->g_w.as<double>(); g.g_lj = ctx->g_lj.as<double>(); g.g_q = ctx->g_q.as<double>();
     g.g_k = ctx->g_k.as<double>(); g.frac = B->frac64; g.kpref2 = B->kpref2;
     g.lj_only = grad->lj_only != 0 ? 1 : 0;
+    g.skip_lj = 1;
     {
         Timer tm(ctx, 5);
-        pa::k_heavy<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, ca, g);
+        // LJ: every survivor's weighted per-run sums from the forward pass
+        pa::Work wi{};
+        wi.sorted = ctx->item_sorted.as<int32_t>(); wi.bin_start = ctx->item_bin_start.as<int32_t>();
+        wi.tile_start = ctx->item_tile_start.as<int32_t>(); wi.counters = ctx->counters.as<int32_t>() + 8;
+        w.item_pq = ctx->item_pq.as<float2>();
+        PA_DISPATCH_NS(N, (pa::k_lj_reduce<NSV><<<unsigned(ctx->num_sms * 8), 256, 0, st>>>(B->d32, ca, wi, w, g)));
         PA_CUDA(ctx, cudaGetLastError());
-        cudaError_t e = cudaSuccess;
-        PA_DISPATCH_NS(N, (e = launch_grad<NSV>(B, ca, w, g, ctx->num_sms, st)));
-        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("adjoint kernel launch: ") + cudaGetErrorString(e));
-        int nl = 2;
+        int nl = 1;
+        if (!g.lj_only) {  // charges: the heavy insertions recomputed
+            pa::k_heavy<<<unsigned((n_act + 255) / 256), 256, 0, st>>>(w, ca, g);
+            PA_CUDA(ctx, cudaGetLastError());
+            cudaError_t e = cudaSuccess;
+            PA_DISPATCH_NS(N, (e = launch_grad<NSV>(B, ca, w, g, ctx->num_sms, st)));
+            if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("adjoint kernel launch: ") + cudaGetErrorString(e));
+            nl += 2;
+        }
         if (B->nk > 0 && !g.lj_only) {
             int32_t amax = 0;
             for (int fw = 0; fw < B->nfw; ++fw) amax = std::max(amax, B->atom_offsets[fw + 1] - B->atom_offsets[fw]);

@@ -65,8 +65,9 @@ __device__ __forceinline__ void bin_centre(const DevBatch<float>& b, int32_t fw,
     cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
 }
 
-// EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms.
-template <int NS, bool EQCUT>
+// EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms. PQ: also store each
+// item's LJ sums per type run (w.item_pq) for the adjoint.
+template <int NS, bool EQCUT, bool PQ>
 __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[PA_WARPS32][2];
@@ -138,6 +139,8 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         const int2* runs = b.list_runs + int64_t(bin) * b.runs_per_bin;
         int32_t ri = 0, rnext = runs[1].x;
         float sg = s_sig2[as * nt + runs[0].y], ep = s_eps4[as * nt + runs[0].y];
+        float sp = 0.f, sq = 0.f;  // PQ: the current run's Σ x(x-1) and Σ x(2x-1)
+        float2* runsums = PQ ? w.item_pq + int64_t(lo + lane) * b.runs_per_bin : nullptr;
         // tmo_at: chunk whose copy did not arrive in time (-1: none); after it no copies are issued
         // and only the chunk already in flight is still waited for
         int32_t tmo_at = -1;
@@ -166,7 +169,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                 if (EQCUT || r2 < rl2) {
                                     const float x = sg * (ri * ri);
                                     const float x3 = x * x * x;
-                                    e = ep * (x3 * x3 - x3);
+                                    const float u = x3 * x3 - x3;
+                                    e = ep * u;
+                                    if (PQ) { sp += u; sq = fmaf(x3, x3, sq + u); }
                                 }
                                 if (EQCUT || r2 < re2) {
                                     const float z = alpha * (r2 * ri);
@@ -180,13 +185,19 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                             } else {
                                 const float x = sg * rcp_nr(r2);
                                 const float x3 = x * x * x;
-                                e = ep * (x3 * x3 - x3);
+                                const float u = x3 * x3 - x3;
+                                e = ep * u;
+                                if (PQ) { sp += u; sq = fmaf(x3, x3, sq + u); }
                             }
                             kahan_add(esum, ecmp, e);
                         }
                     }
                     if (j >= n) break;
                     // entry j starts the next type run
+                    if (PQ) {
+                        if (active) runsums[ri] = make_float2(sp, sq);
+                        sp = 0.f; sq = 0.f;
+                    }
                     ++ri;
                     const int32_t ty = runs[ri].y;
                     rnext = runs[ri + 1].x;
@@ -207,6 +218,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             if (lane == 0) atomicExch(&w.counters[2], 1);
             return;
         }
+        if (PQ && active && nch > 0) runsums[ri] = make_float2(sp, sq);  // the last run
         if (active) w.dUs[it] = double(esum) - double(ecmp);
     }
 }

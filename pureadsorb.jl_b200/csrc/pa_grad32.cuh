@@ -25,6 +25,7 @@ struct GradArgs {
     const int64_t* sys_koff;  // nsys+1: each system's first k slot
     int32_t nsys;
     int32_t lj_only;          // nonzero: no charge derivatives (real-space terms, G_k)
+    int32_t skip_lj;          // nonzero: k_grad32 leaves the LJ sums (k_lj_reduce forms them)
     int32_t* heavy;           // n_act: local indices of the recomputed insertions
     int32_t* nheavy;          // count of heavy
     double* g_w;              // nsys: Σ w over the recomputed insertions
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
                 }
                 const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
                 const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                if (r2 < rl2) {
+                if (!g.skip_lj && r2 < rl2) {
                     const float x = s_sig2[s * nt + ty] * rcp_nr(r2);
                     const float x3 = x * x * x;
                     P = fmaf(x3, x3 - 1.0f, P);
@@ -177,6 +178,66 @@ __global__ void __launch_bounds__(32 * PA_WARPSG) k_grad32(DevBatch<float> b, Ca
             }
         }
         if (lane == 0) atomicAdd(&g.g_w[sy], wgt);
+    }
+}
+
+// The LJ part of the adjoint from the forward pass's per-run sums (w.item_pq): per tile of 32
+// sorted items of one bin, each item's weight w = exp(-ΔU/kT - m_s) times its runs' sums, reduced
+// over the warp per (guest site, run) in a fixed order and added to the system's
+// [s][0 or 1][site][type of the run] sums. Tiles are taken in order, warp by warp; every survivor
+// enters (weights far below the largest underflow to zero).
+template <int NS>
+__global__ void __launch_bounds__(256) k_lj_reduce(DevBatch<float> b, CallArgs ca, Work wi, Work w, GradArgs g) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int32_t total = wi.counters[1];
+    const int nt = b.ntypes, rm = b.runs_per_bin, nacc = 2 * NS * nt;
+    const unsigned FULL = 0xffffffffu;
+    for (int64_t t = warp; t < total; t += nwarps) {
+        const int32_t bin = find_bin(wi.tile_start, b.nbins, int32_t(t));
+        const int32_t lo = wi.bin_start[bin] + (int32_t(t) - wi.tile_start[bin]) * PA_TILE32;
+        const int32_t hi = min(lo + PA_TILE32, wi.bin_start[bin + 1]);
+        const bool active = lo + lane < hi;
+        const int32_t it = active ? wi.sorted[lo + lane] : 0;
+        const int32_t li = it / NS, as = it - li * NS;
+        const int32_t s = find_system(ca.sys_off, g.nsys, ca.i_lo + li);
+        double wgt = 0.0;
+        if (active) {
+            const double x = -w.dU[li] / g.kT;
+            if (x > -INFINITY) wgt = exp(x - g.xmax[s]);
+        }
+        const int32_t s0 = __shfl_sync(FULL, s, 0);
+        const bool one = __all_sync(FULL, !active || s == s0);
+        const int32_t l1 = b.list_offsets[bin + 1];
+        const int2* runs = b.list_runs + int64_t(bin) * rm;
+        const float2* pq = w.item_pq + int64_t(lo + lane) * rm;
+        for (int32_t r = 0; r < rm; ++r) {
+            const int2 run = runs[r];
+            if (run.x >= l1) break;  // (warp-uniform) past the bin's last run
+            float2 v = active ? pq[r] : make_float2(0.f, 0.f);
+            const double vp = wgt * double(v.x), vq = wgt * double(v.y);
+            if (one) {
+#pragma unroll
+                for (int a = 0; a < NS; ++a) {
+                    double p = as == a ? vp : 0.0, q = as == a ? vq : 0.0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        p += __shfl_xor_sync(FULL, p, o);
+                        q += __shfl_xor_sync(FULL, q, o);
+                    }
+                    if (lane == 0) {
+                        double* acc = g.g_lj + int64_t(s0) * nacc;
+                        if (p != 0.0) atomicAdd(&acc[a * nt + run.y], p);
+                        if (q != 0.0) atomicAdd(&acc[(NS + a) * nt + run.y], q);
+                    }
+                }
+            } else if (active) {  // a tile spanning systems that share a framework
+                double* acc = g.g_lj + int64_t(s) * nacc;
+                if (vp != 0.0) atomicAdd(&acc[as * nt + run.y], vp);
+                if (vq != 0.0) atomicAdd(&acc[(NS + as) * nt + run.y], vq);
+            }
+        }
     }
 }
 

@@ -111,6 +111,9 @@ struct Work {
     double* dUs;          // n_act*NS: real-space energy of each item's site
     double* dUr;          // n_act: KE times the reciprocal cross term
     double* dUg;          // n_act: guest-guest real-space term (insertion along a chain), else NULL
+    // with the adjoint: per sorted item and type run of its bin's list, the LJ sums (Σ x(x-1),
+    // Σ x(2x-1)), x = (sigma/r)^6, over the item's pairs inside the LJ cutoff (else NULL)
+    float2* item_pq;
 };
 
 // ---------------------------------------------------------------------------------------------

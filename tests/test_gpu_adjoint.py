@@ -114,7 +114,7 @@ def test_lj_only_mode_keeps_lj_gradients(pa, backend, case):
     lj, gl = pa.widom_grad(b32, case.guest, case.ff, T=298.15, ninsert=NINS, backend=backend, seed=SEED,
                            nblocks=NBLOCKS, run=RUN, charges=False)
     assert gl[0].charges is None
-    assert gl[0].recomputed == gf[0].recomputed
+    assert gl[0].recomputed == 0 and gf[0].recomputed > 0
     assert lj[0].K_H == full[0].K_H
     for name in ("epsilon", "sigma"):
         a, f = getattr(gl[0], name), getattr(gf[0], name)
