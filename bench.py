@@ -26,9 +26,10 @@ import __graft_entry__ as ge  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
-# DRAM bytes (read + write) of one k_energy32 launch on this workload, from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
-ENERGY32_TRAFFIC_BYTES = 96.518656e6 + 8.461312e6
+# DRAM bytes (read + write) of one k_energy32 launch on this workload with 3.5 Å bins, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
+ENERGY32_TRAFFIC_BYTES = 69.985792e6 + 8.245248e6
+ENERGY32_TRAFFIC_BIN_WIDTH = 3.5
 
 
 def parse():
@@ -45,6 +46,7 @@ def parse():
     p.add_argument("--no-fit", action="store_true")
     p.add_argument("--no-chain", action="store_true")
     p.add_argument("--no-tune", action="store_true", help="default bin width and grid (e.g. for profiling)")
+    p.add_argument("--bin-width", type=float, default=0.0, help="with --no-tune: this bin width (Å) instead of 3.0")
     return p.parse_args()
 
 
@@ -383,7 +385,10 @@ def main():
     # layout and launch shape chosen by the autotuner on this rank's own call, then every step
     # replayed from a CUDA graph
     if args.no_tune:
-        tune = pa.TuneReport(3.0, 8, float("nan"), [])
+        bw = args.bin_width if args.bin_width > 0 else 3.0
+        ctx.set_tuning(bin_width=bw, ctas_per_sm=8)
+        batch.drop_device()
+        tune = pa.TuneReport(bw, 8, float("nan"), [])
     else:
         tune = pa.autotune(batch, guest, T=prm["T"], ninsert=args.ninsert, backend=backend, seed=prm["seed"],
                            nblocks=nblocks)
@@ -463,7 +468,8 @@ def main():
         peak = fp32_peak(torch)
         ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": ENERGY32_TRAFFIC_BYTES if args.ninsert == 1_000_000 and world == 1 else None,
+                "traffic": ENERGY32_TRAFFIC_BYTES if (args.ninsert == 1_000_000 and world == 1
+                                                      and tune.bin_width == ENERGY32_TRAFFIC_BIN_WIDTH) else None,
                 "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
                 "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
                 "flops_per_survivor": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
