@@ -76,7 +76,8 @@ struct pa_context {
     std::vector<unsigned char> gkey, last_key;  // key of the captured graph, and of the last call
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
     // counters, and host copies of the last uploaded per-call tables (re-uploaded only on change)
-    DevMem scal, bnd;
+    DevMem scal, bnd, rho2max;
+    std::vector<unsigned char> up_rho2max;
     double* h_seg = nullptr;
     size_t h_seg_cap = 0;
     int32_t* h_cnt = nullptr;
@@ -979,6 +980,16 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         if (f32) { float* p = reinterpret_cast<float*>(r2.data()); for (int64_t q = 0; q < nr; ++q) p[q] = float(args->rho2[q]); }
         else std::memcpy(r2.data(), args->rho2, nr * sizeof(double));
         PA_CUDA(ctx, upload_cached(ctx->rho2, ctx->up_rho2, r2, st));
+        // each (system, site)'s largest radius squared, in the kernels' type (phase 0's pre-test)
+        const int64_t nm = int64_t(nsys) * N;
+        std::vector<unsigned char> rm(nm * (f32 ? sizeof(float) : sizeof(double)));
+        for (int64_t q = 0; q < nm; ++q) {
+            double m = 0;
+            for (int t = 0; t < nt; ++t) m = std::max(m, args->rho2[q * nt + t]);
+            if (f32) reinterpret_cast<float*>(rm.data())[q] = float(m);
+            else reinterpret_cast<double*>(rm.data())[q] = m;
+        }
+        PA_CUDA(ctx, upload_cached(ctx->rho2max, ctx->up_rho2max, rm, st));
     }
     {
         const uint64_t seed = args->seed;
@@ -1063,6 +1074,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     ca.reject = args->reject ? 1 : 0; ca.kT = args->kT;
     ca.seed_dev = ctx->scal.as<uint64_t>(); ca.kT_dev = ctx->scal.as<double>() + 1;
     ca.k_offset = chain ? chain->k_offset : 0; ca.koff_dev = reinterpret_cast<const int64_t*>(ctx->scal.as<double>() + 2);
+    ca.rho2max = args->reject ? ctx->rho2max.p : nullptr;
     {
         cudaError_t e = cudaSuccess;
         PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));

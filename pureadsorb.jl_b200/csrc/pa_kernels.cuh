@@ -82,6 +82,9 @@ struct CallArgs {
     // follow the previous cycles'); koff_dev, when set, is read instead (graph replays)
     int64_t k_offset;
     const int64_t* koff_dev;
+    // optional (F-typed, nsys*N): each (system, site)'s largest rejection radius squared, for
+    // phase 0's relaxed pre-test; NULL: every atom of the stencil takes the strict test
+    const void* rho2max;
 };
 
 __device__ __forceinline__ int64_t k_shift(const CallArgs& ca) { return ca.koff_dev ? *ca.koff_dev : ca.k_offset; }
@@ -147,7 +150,7 @@ __device__ __forceinline__ void kahan_add(float& sum, float& c, float x) {
 // oracle's hardcore_flag).
 template <typename F, int NS>
 __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const F* rp, const F* qt,
-                              const F* rho2, const int32_t* reach0) {
+                              const F* rho2, const int32_t* reach0, const F* rho2max) {
     typedef St<F> S;
     const F* A = b.cells + 9 * fw;
     const F* iA = b.invcells + 9 * fw;
@@ -162,6 +165,14 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
     F pos[3];
     matvec_s(Ael, rp, pos);
     const F* r2row = rho2 + int64_t(s) * NS * nt;
+    // Relaxed pre-test. Inside the stencil every atom is visited at the image of its unwrapped
+    // cell, i.e. at its stored position plus A w, w the row's wrap (-1, 0 or 1 per axis). With the
+    // stencil narrower than the grid on every axis, that image lies within a few cells of the site,
+    // so it is the strict minimum image whenever the atom is within reach (any other image is at
+    // least half a cell width away). Its distance in plain FP32/FP64 arithmetic differs from the
+    // strict one by rounding only, far below the 1e-3 A^2 margin, so an atom at least the site's
+    // largest radius squared plus the margin away cannot set the flag and skips the strict test.
+    const bool pre = rho2max != nullptr && 2 * m1 + 1 < n1 && 2 * m2 + 1 < n2 && 2 * m3 + 1 < n3;
 #pragma unroll 1
     for (int a = 0; a < NS; ++a) {
         F g[3];
@@ -177,6 +188,12 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
         stencil_start_count(h2, m2, n2, &st2, &c2);
         stencil_start_count(h3, m3, n3, &st3, &c3);
         const F* r2a = r2row + a * nt;
+        const F lim = pre ? rho2max[int64_t(s) * NS + a] + F(1e-3) : F(0);
+        // the site in its home cell's periodic frame, sp - A floor(f)
+        const F fl0 = floor(f[0]), fl1 = floor(f[1]), fl2 = floor(f[2]);
+        const F bx = sp[0] - (Ael[0] * fl0 + Ael[3] * fl1 + Ael[6] * fl2);
+        const F by = sp[1] - (Ael[1] * fl0 + Ael[4] * fl1 + Ael[7] * fl2);
+        const F bz = sp[2] - (Ael[2] * fl0 + Ael[5] * fl1 + Ael[8] * fl2);
         // The x-cells of one (y, z) row of the stencil are consecutive in the cell-sorted atom
         // array, so each row is one contiguous atom range, or two where it wraps around the grid.
         // Atoms are visited in the same order as cell by cell (x innermost).
@@ -185,14 +202,25 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
         const int32_t xb1 = st1 < 0 ? st1 + c1 : max(st1 + c1 - n1, 0);
         for (int32_t t3 = 0; t3 < c3; ++t3) {
             const int32_t z = wrap_cell(st3 + t3, n3);
+            const F wz = F((st3 + t3 < 0) ? -1 : (st3 + t3 >= n3 ? 1 : 0));
             for (int32_t t2 = 0; t2 < c2; ++t2) {
                 const int32_t row = n1 * (wrap_cell(st2 + t2, n2) + n2 * z);
+                const F wy = F((st2 + t2 < 0) ? -1 : (st2 + t2 >= n2 ? 1 : 0));
                 // part A: cells [xa0, xa1); part B (wrapped): cells [0, xb1)
                 for (int part = 0; part < 2; ++part) {
                     const int32_t j0 = a0 + coff[row + (part == 0 ? xa0 : 0)];
                     const int32_t j1 = a0 + coff[row + (part == 0 ? xa1 : xb1)];
+                    const F wx = F(part == 0 ? (st1 < 0 ? -1 : 0) : (st1 < 0 ? 0 : 1));
+                    // the site relative to this row part's atom images: b - A w
+                    const F ex = bx - (Ael[0] * wx + Ael[3] * wy + Ael[6] * wz);
+                    const F ey = by - (Ael[1] * wx + Ael[4] * wy + Ael[7] * wz);
+                    const F ez = bz - (Ael[2] * wx + Ael[5] * wy + Ael[8] * wz);
                     for (int32_t j = j0; j < j1; ++j) {
                         typename Vec4<F>::T at = b.atoms[j];
+                        if (pre) {
+                            const F dx = ex - at.x, dy = ey - at.y, dz = ez - at.z;
+                            if (dx * dx + dy * dy + dz * dz >= lim) continue;
+                        }
                         F D[3] = {S::sub(sp[0], at.x), S::sub(sp[1], at.y), S::sub(sp[2], at.z)};
                         minimum_image_s(Ael, iAel, D);
                         F r2 = dot3s(D[0], D[1], D[2], D[0], D[1], D[2]);
@@ -295,7 +323,7 @@ __global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Wor
         w.pose64a[t] = make_double4(double(rp[0]), double(rp[1]), double(rp[2]), 0.0);
         w.pose64b[t] = make_double4(double(qt[0]), double(qt[1]), double(qt[2]), double(qt[3]));
     }
-    if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0)) {
+    if (ca.reject && hardcore_scan<F, NS>(b, s, fw, rp, qt, rho2, reach0, static_cast<const F*>(ca.rho2max))) {
         mark_rejected(w, t, NS);
         return;
     }
@@ -336,7 +364,7 @@ __global__ void __launch_bounds__(256, 4) k_phase0_32(DevBatch<float> b, CallArg
     const int32_t fw = b.framework_of[s];
     const float4 pa = w.pose_a[t], pq = w.pose_b[t];
     const float rp[3] = {pa.x, pa.y, pa.z}, qt[4] = {pq.x, pq.y, pq.z, pq.w};
-    if (ca.reject && hardcore_scan<float, NS>(b, s, fw, rp, qt, rho2, reach0)) {
+    if (ca.reject && hardcore_scan<float, NS>(b, s, fw, rp, qt, rho2, reach0, static_cast<const float*>(ca.rho2max))) {
         mark_rejected(w, t, NS);
         return;
     }
