@@ -294,8 +294,11 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
                     row = 0.f;
 #pragma unroll
                     for (int s = 0; s < NS; ++s) {
-                        const float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
-                        sincospif(2.0f * ph, &ci[s], &cr[s]);
+                        // the phase reduced to [-1/2, 1/2] turns, then the hardware sine and
+                        // cosine (absolute error about 4e-7 on [-pi, pi])
+                        float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
+                        ph -= rintf(ph);
+                        __sincosf(6.28318530717958648f * ph, &ci[s], &cr[s]);
                     }
                 } else {  // next k-vector of the row
 #pragma unroll
