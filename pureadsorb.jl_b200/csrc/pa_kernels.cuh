@@ -206,8 +206,9 @@ __device__ bool hardcore_scan(const DevBatch<F>& b, int32_t s, int32_t fw, const
             for (int32_t t2 = 0; t2 < c2; ++t2) {
                 const int32_t row = n1 * (wrap_cell(st2 + t2, n2) + n2 * z);
                 const F wy = F((st2 + t2 < 0) ? -1 : (st2 + t2 >= n2 ? 1 : 0));
-                // part A: cells [xa0, xa1); part B (wrapped): cells [0, xb1)
-                for (int part = 0; part < 2; ++part) {
+                // part A: cells [xa0, xa1); part B (wrapped, empty unless the stencil crosses the
+                // grid's x boundary): cells [0, xb1)
+                for (int part = 0; part < (xb1 > 0 ? 2 : 1); ++part) {
                     const int32_t j0 = a0 + coff[row + (part == 0 ? xa0 : 0)];
                     const int32_t j1 = a0 + coff[row + (part == 0 ? xa1 : xb1)];
                     const F wx = F(part == 0 ? (st1 < 0 ? -1 : 0) : (st1 < 0 ? 0 : 1));
