@@ -169,7 +169,7 @@ def chain_workload(pa, orc, backend, torch, stream, flush, no_cpu=False):
     ctx = backend.ctx
     fws, ff, guest, ewald, prm = pa.synthetic.co2(T=np.float32)
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws * 2, ff, guest, ewald, fullk=True)
+    b = pa.FrameworkBatch(fws * 2, ff, guest, ewald, fullk=True, sk=ctx.structure_factor, self_term=ctx.self_term)
     st = pa.SystemState.placed(b, guest, [10, 40], T=prm["T"], seed=1001)
     build_s = time.perf_counter() - t0
     nper, T, seed = 2**18, prm["T"], prm["seed"]
@@ -243,7 +243,7 @@ def batched_workload(pa, backend, torch, stream, flush):
     ctx = backend.ctx
     fws, ff, guest, ewald, prm = pa.synthetic.batched(T=np.float32)
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws, ff, guest, ewald, sk=ctx.structure_factor)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, sk=ctx.structure_factor, self_term=ctx.self_term)
     build_s = time.perf_counter() - t0
     n, T, seed, nb = prm["ninsert"], prm["T"], prm["seed"], prm["nblocks"]
     tune = pa.autotune(b, guest, T=T, ninsert=n, backend=backend, seed=seed, nblocks=nb, bin_widths=(3.0, 3.5, 4.0),
@@ -273,7 +273,7 @@ def batched_workload(pa, backend, torch, stream, flush):
         UW = sUW.reshape(len(fws), nb).sum(axis=1)
         return W, UW
 
-    b64 = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float64, sk=ctx.structure_factor)
+    b64 = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float64, sk=ctx.structure_factor, self_term=ctx.self_term)
     raw(b64)
     torch.cuda.synchronize()
     a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -308,10 +308,10 @@ def fitting_workload(pa, backend):
     t0 = time.perf_counter()
     ffh = pa.fit.scaled_forcefield(ff, prm["fitted_types"], prm["hidden"])
     targets = pa.fit.target_lnkh(fws, ffh, guest, ewald, T=T, ninsert=n, seed=seed, backend=backend,
-                                 sk=ctx.structure_factor)
+                                 sk=ctx.structure_factor, self_term=ctx.self_term)
     target_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor, self_term=ctx.self_term)
     build_s = time.perf_counter() - t0
     res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
                                lr=prm["lr"], seed=seed, backend=backend)

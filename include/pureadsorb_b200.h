@@ -283,6 +283,12 @@ pa_status pa_pose_host(int32_t precision, uint64_t seed, uint64_t s, uint64_t k,
 pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, const double* positions,
                               const double* charges, int64_t natoms, double* S);
 
+/* Guest self term of the batch's constant offset for a set of orientations (src/batch.jl:357-375):
+ * samples[o] = Σ_k kpref_k |Σ_s q_s exp(i k·g_s(o))|^2 over the given k-vectors, in FP64 on the
+ * device (without the KE factor). sites: norient*nguest*3 rotated body-frame site offsets. */
+pa_status pa_self_term(pa_context* ctx, const double* ks, const double* kpref, int64_t nk, const double* sites,
+                       const double* charges, int32_t nguest, int32_t norient, double* samples);
+
 /* Library version string. */
 const char* pa_version(void);
 

@@ -92,6 +92,7 @@ SIGNATURES = [
     ("pa_segment_count", _i32, [_i64, _i32, _i32, _i32, ctypes.POINTER(_i64)]),
     ("pa_combine_segments", _i32, [_i64, _i32, _i32, _i32, _p, ctypes.POINTER(BlockSums)]),
     ("pa_pose_host", _i32, [_i32, _u64, _u64, _u64, _p, _p]),
+    ("pa_self_term", _i32, [_p, _p, _p, _i64, _p, _p, _i32, _i32, _p]),
     ("pa_structure_factor", _i32, [_p, _p, _i64, _p, _p, _i64, _p]),
     ("pa_version", ctypes.c_char_p, []),
 ]
@@ -204,6 +205,19 @@ class Context:
         n = np.zeros(8, dtype=np.int64)
         self.check(lib().pa_context_kernel_times(self.handle, ptr(ms), ptr(n)), "pa_context_kernel_times")
         return ms, n
+
+    def self_term(self, ks, kpref, sites, charges):
+        """Σ_k kpref |Σ_s q_s e^{i k·g_s(o)}|^2 for every orientation o of `sites` (norient x N x 3),
+        on the device (pa_self_term)."""
+        ks = np.ascontiguousarray(ks, dtype=np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(kpref, dtype=np.float64)
+        g = np.ascontiguousarray(sites, dtype=np.float64)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        no, N = g.shape[0], g.shape[1]
+        out = np.zeros(no)
+        self.check(lib().pa_self_term(self.handle, ptr(ks), ptr(w), len(ks), ptr(g), ptr(q), N, no, ptr(out)),
+                   "pa_self_term")
+        return out
 
     def structure_factor(self, ks, positions, charges):
         ks = np.ascontiguousarray(ks, dtype=np.float64).reshape(-1, 3)

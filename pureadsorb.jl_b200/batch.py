@@ -70,10 +70,12 @@ class FrameworkBatch:
 
     `sk`, if given, computes host structure factors (ks, positions, charges) -> complex array;
     the default evaluates them on the host in FP64 like the reference, and
-    `sk=Context.structure_factor` runs the library's FP64 device kernel instead.
+    `sk=Context.structure_factor` runs the library's FP64 device kernel instead. `self_term`,
+    likewise, computes the guest self term's per-orientation sums (ks, kpref, sites, charges) ->
+    array (without KE); `self_term=Context.self_term` runs them on the device.
     """
 
-    def __init__(self, fws, ff, guest, ewald, cellwidth=2, fullk=False, T=None, sk=None):
+    def __init__(self, fws, ff, guest, ewald, cellwidth=2, fullk=False, T=None, sk=None, self_term=None):
         fws = list(fws)
         if not fws:
             raise ArgumentError("FrameworkBatch needs at least one framework")
@@ -172,12 +174,15 @@ class FrameworkBatch:
                 kpref.append(kpref_full[sel])
                 Shost.append(Sh_full[sel])
                 kcoeffs.append(coeffs[sel])
-                samples = np.empty(SELF_TERM_NORIENT)
-                for o in range(SELF_TERM_NORIENT):
-                    gs = self_sites[o]
-                    ph = kv_full @ gs.T
-                    Sg = np.cos(ph) @ guest.charges + 1j * (np.sin(ph) @ guest.charges)
-                    samples[o] = KE * float(np.sum(kpref_full * np.abs(Sg) ** 2))
+                if self_term is not None:
+                    samples = KE * np.asarray(self_term(kv_full, kpref_full, self_sites, guest.charges))
+                else:
+                    samples = np.empty(SELF_TERM_NORIENT)
+                    for o in range(SELF_TERM_NORIENT):
+                        gs = self_sites[o]
+                        ph = kv_full @ gs.T
+                        Sg = np.cos(ph) @ guest.charges + 1j * (np.sin(ph) @ guest.charges)
+                        samples[o] = KE * float(np.sum(kpref_full * np.abs(Sg) ** 2))
                 self_mean = float(np.sum(samples)) / len(samples)
                 half = (float(np.max(samples)) - float(np.min(samples))) / 2
                 halfranges.append(half)

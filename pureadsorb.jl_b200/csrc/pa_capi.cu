@@ -1431,6 +1431,31 @@ pa_status pa_pose_host(int32_t precision, uint64_t seed, uint64_t s, uint64_t k,
     return PA_OK;
 }
 
+pa_status pa_self_term(pa_context* ctx, const double* ks, const double* kpref, int64_t nk, const double* sites,
+                       const double* charges, int32_t nguest, int32_t norient, double* samples) {
+    if (!ctx || !samples || norient < 1 || nguest < 1 || !sites || !charges || (nk > 0 && (!ks || !kpref)))
+        return fail(ctx, PA_ERR_ARG, "null argument");
+    if (nk == 0) {
+        for (int32_t o = 0; o < norient; ++o) samples[o] = 0.0;
+        return PA_OK;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    DevMem dk, dw, dg, dq, dout;
+    std::vector<double> vk(ks, ks + 3 * nk), vw(kpref, kpref + nk), vg(sites, sites + 3 * int64_t(nguest) * norient),
+        vq(charges, charges + nguest);
+    PA_CUDA(ctx, upload(dk, vk, st));
+    PA_CUDA(ctx, upload(dw, vw, st));
+    PA_CUDA(ctx, upload(dg, vg, st));
+    PA_CUDA(ctx, upload(dq, vq, st));
+    PA_CUDA(ctx, dout.ensure(sizeof(double) * norient));
+    pa::k_self_term<<<unsigned(norient), 256, 0, st>>>(dk.as<double>(), dw.as<double>(), nk, dg.as<double>(),
+                                                     dq.as<double>(), nguest, dout.as<double>());
+    PA_CUDA(ctx, cudaGetLastError());
+    PA_CUDA(ctx, cudaMemcpyAsync(samples, dout.p, sizeof(double) * norient, cudaMemcpyDeviceToHost, st));
+    return wait_stream(ctx);
+}
+
 pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, const double* positions,
                               const double* charges, int64_t natoms, double* S) {
     if (!ctx || (nk > 0 && (!ks || !S)) || (natoms > 0 && (!positions || !charges))) return fail(ctx, PA_ERR_ARG, "null argument");

@@ -896,6 +896,35 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
     }
 }
 
+// Guest self term per orientation (src/batch.jl:357-375): one CTA per orientation o, threads over
+// the k-vectors, Σ_k kpref_k |Σ_s q_s e^{i k·g_s(o)}|^2 in FP64, per-thread partial sums then a
+// fixed tree over the CTA.
+__global__ void __launch_bounds__(256) k_self_term(const double* ks, const double* kpref, int64_t nk,
+                                                   const double* sites, const double* q, int32_t N, double* out) {
+    __shared__ double s_red[256];
+    const int32_t o = blockIdx.x;
+    const double* g = sites + int64_t(o) * N * 3;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < nk; i += blockDim.x) {
+        const double kx = ks[3 * i], ky = ks[3 * i + 1], kz = ks[3 * i + 2];
+        double re = 0.0, im = 0.0;
+        for (int32_t s = 0; s < N; ++s) {
+            double sn, cs;
+            sincos(kx * g[3 * s] + ky * g[3 * s + 1] + kz * g[3 * s + 2], &sn, &cs);
+            re += q[s] * cs;
+            im += q[s] * sn;
+        }
+        acc += kpref[i] * (re * re + im * im);
+    }
+    s_red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (int(threadIdx.x) < w) s_red[threadIdx.x] += s_red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[o] = s_red[0];
+}
+
 // FP64 structure factor: one thread per k-vector, sequential sum over atoms (src/ewald.jl:159-170).
 __global__ void __launch_bounds__(256) k_structure_factor(const double* ks, int64_t nk, const double* pos,
                                                           const double* q, int64_t na, double* S) {

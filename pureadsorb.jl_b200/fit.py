@@ -35,10 +35,10 @@ def scaled_forcefield(ff, types, x):
     return ForceField(ff.names, sig, eps, cutoff=ff.cutoff, tail=ff.tail)
 
 
-def target_lnkh(fws, ff, guest, ewald, *, T, ninsert, seed, nblocks=10, backend=None, sk=None):
+def target_lnkh(fws, ff, guest, ewald, *, T, ninsert, seed, nblocks=10, backend=None, sk=None, self_term=None):
     """ln K_H of every framework from the plain FP64 path (the reference algorithm) at ff; -inf
     for a framework without accessible volume (every sampled weight zero)."""
-    b64 = FrameworkBatch(fws, ff, guest, ewald, T=np.float64, sk=sk)
+    b64 = FrameworkBatch(fws, ff, guest, ewald, T=np.float64, sk=sk, self_term=self_term)
     lse, sw, suw, cnt = _widom(b64, guest, reject=True, T=T, ninsert=ninsert, seed=seed, nblocks=nblocks,
                                backend=backend, segment_range=(0, 0))
     kT = float(b64.T(KB * float(T)))
