@@ -77,7 +77,7 @@ def fit_lj_scales(batch, guest, ff, types, targets, *, T, ninsert, steps=200, lr
         lnk, grads = widom_grad(b, guest, ffx, T=T, ninsert=ninsert, backend=backend, seed=seed, nblocks=nblocks,
                                 reduce=False, charges=False)
         use = np.isfinite(lnk) & np.isfinite(targets)
-        r = (lnk - targets)[use]
+        r = lnk[use] - targets[use]
         g_eps = np.array([g.epsilon[idx] for g, u in zip(grads, use) if u]) * eps0[idx]
         g_sig = np.array([g.sigma[idx] for g, u in zip(grads, use) if u]) * sig0[idx]
         grad = np.concatenate([2 * (r[:, None] * g_eps).mean(axis=0), 2 * (r[:, None] * g_sig).mean(axis=0)])
