@@ -30,6 +30,9 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM 
 # capture (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
 ENERGY32_TRAFFIC_BYTES = 69.985792e6 + 8.245248e6
 ENERGY32_TRAFFIC_BIN_WIDTH = 3.5
+# the metric and workload names of both arms (ours and the reference's CPU implementation)
+METRIC = "Widom insertions/s (CO2, 5,832-atom framework)"
+WORKLOAD = "co2_5832_atoms_3x3x3_monoclinic"
 
 
 def parse():
@@ -343,10 +346,10 @@ def main():
             if i >= args.warmup:
                 rates.append(r)
         v = float(np.median(rates))
-        line = {"metric": "Widom insertions/s (CO2, 5,832-atom framework)", "value": v, "unit": "insertions/s",
+        line = {"metric": METRIC, "value": v, "unit": "insertions/s",
                 "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "co2_5832_atoms", "ninsert": args.ninsert, "sample_insertions": n},
+                "config": {"workload": WORKLOAD, "ninsert": args.ninsert, "sample_insertions": n},
                 "cpu_baseline": {"value": v, "unit": "insertions/s", "cores": cores, "kind": "port",
                                  "sample": f"{n} insertions of the workload per step (two-phase, FP64)"},
                 "e2e": {"value": v, "unit": "insertions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -553,11 +556,11 @@ def main():
             cpu = {"value": r, "unit": "insertions/s", "cores": cores, "kind": "port",
                    "sample": f"{n} insertions of the workload (FP64 oracle, two-phase, OpenMP)"}
 
-        line = {"metric": "Widom insertions/s (CO2, 5,832-atom framework), FP32 form",
+        line = {"metric": METRIC,
                 "value": value, "unit": "insertions/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "co2_5832_atoms_3x3x3_monoclinic", "ninsert_per_gpu": args.ninsert,
+                "config": {"workload": WORKLOAD, "ninsert_per_gpu": args.ninsert,
                            "ninsert_total": ninsert, "natoms": int(len(batch.positions)), "guest_sites": 3,
                            "coupled_k": nk, "nblocks": nblocks, "seed": prm["seed"], "T_K": prm["T"],
                            "l2": "flushed between steps (256 MB write)", "parallelism": f"shard{world}"},
