@@ -115,10 +115,16 @@ class FrameworkBatch:
                       else None)
 
         # compact LJ types: framework atoms' types union the guest's (src/batch.jl:309-317)
-        ty_orig = [np.array([ff.typeindex(s + "_") for s in fw.symbols], dtype=np.int64) for fw in unique]
+        ty_orig = []
+        for fw in unique:  # one lookup per distinct symbol, then a gather over the atoms
+            syms, inv = np.unique(np.asarray(fw.symbols, dtype=str), return_inverse=True)
+            idx = np.array([ff.typeindex(s + "_") for s in syms], dtype=np.int64)
+            ty_orig.append(idx[inv.reshape(-1)] if len(syms) else np.zeros(0, np.int64))
         allt = np.concatenate(ty_orig + [np.asarray(guest.types, dtype=np.int64)])
         compact_to_orig = np.unique(allt).astype(np.int32)
         o2c = {int(t): i + 1 for i, t in enumerate(compact_to_orig)}
+        o2c_arr = np.zeros(int(compact_to_orig.max(initial=0)) + 1, dtype=np.int32)
+        o2c_arr[compact_to_orig] = np.arange(1, len(compact_to_orig) + 1, dtype=np.int32)
         ci = compact_to_orig - 1
         sigma = ff.sigma[np.ix_(ci, ci)].copy()
         epsilon = ff.epsilon[np.ix_(ci, ci)].copy()
@@ -146,7 +152,7 @@ class FrameworkBatch:
             L = perpendicular_lengths(A)
             n_grid = grid_dims(L, w)
             pos = cartesian(fw)
-            ty = np.array([o2c[int(t)] for t in ty_orig[n - 1]], dtype=np.int32)
+            ty = o2c_arr[ty_orig[n - 1]]
             perm, local = cell_sort(fw.frac, n_grid)
             positions.append(pos[perm])
             types.append(ty[perm])
