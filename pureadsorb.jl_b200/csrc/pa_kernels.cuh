@@ -355,17 +355,282 @@ __global__ void __launch_bounds__(256) k_draw32(DevBatch<float> b, CallArgs ca, 
     wa.slot[t] = atomicAdd(&wa.bin_count[fine], 1);
 }
 
+__device__ __forceinline__ int32_t floor_div(int32_t x, int32_t n) { return x >= 0 ? x / n : -((n - 1 - x) / n); }
+
+// k_phase0_32: one warp scans the hard core of 32 consecutive insertions of `order` together.
+// The warp's insertions lie in one or two centre sub-bins, so their per-site stencils (the cells
+// within reach0 of each site's home cell, src/widom.jl:99-151) overlap almost entirely. The warp
+// takes as one region of cells the union, over its sites, of the stencil cells that an atom within
+// the site's largest hard-core radius can occupy (each site's home cell moved by a whole grid
+// period next to the first lane's, so that the region stays compact across the periodic
+// boundary), and stages the atom images of the region in shared memory, 32 at a time; every lane
+// tests its own insertion against each staged atom, so the lanes do the same work, where one
+// stencil walk per lane leaves lanes idle at row boundaries and early exits.
+//
+// Per staged atom a lane first tests the distance to its insertion's centre against the guest's
+// radius plus the largest hard-core radius; only then each site, against the site's largest
+// radius squared plus 1e-3 A^2 (the relaxed pre-test, plain FP32). An atom of a site's stencil is
+// staged at the image of its stencil cell, which is its strict minimum image whenever it is within
+// reach (stencils narrower than the grid), and the plain distances differ from the strict one by
+// rounding only, so no atom that can set the flag is skipped. The pairs that pass are queued and
+// then decided together, one lane per pair: the strict test of hardcore_scan (minimum image, r^2
+// against rho2 of the atom's type), counted only if the atom's cell is in that site's own stencil.
+// The flags are therefore exactly those of the per-site stencil scan. Lanes of another system,
+// stencils as wide as the grid, or a region wider than the grid take hardcore_scan itself.
+#define PA_P0_WARPS 8
+#define PA_P0_QMAX 64
 template <int NS>
-__global__ void __launch_bounds__(256, 4) k_phase0_32(DevBatch<float> b, CallArgs ca, Work w, const int32_t* order,
-                                                      const float* rho2, const int32_t* reach0) {
-    const int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (x >= ca.n_act) return;
-    const int64_t t = order[x];
-    const int32_t s = find_system(ca.sys_off, b.nsys, ca.i_lo + t);
-    const int32_t fw = b.framework_of[s];
-    const float4 pa = w.pose_a[t], pq = w.pose_b[t];
-    const float rp[3] = {pa.x, pa.y, pa.z}, qt[4] = {pq.x, pq.y, pq.z, pq.w};
-    if (ca.reject && hardcore_scan<float, NS>(b, s, fw, rp, qt, rho2, reach0, static_cast<const float*>(ca.rho2max))) {
+__global__ void __launch_bounds__(32 * PA_P0_WARPS, 3) k_phase0_32(DevBatch<float> b, CallArgs ca, Work w,
+                                                                  const int32_t* order, const float* rho2,
+                                                                  const int32_t* reach0) {
+    __shared__ float4 s_img[PA_P0_WARPS][32];          // staged atom images (x, y, z), packed cell
+    __shared__ float4 s_org[PA_P0_WARPS][32];          // the same atoms as stored (x, y, z), type
+    __shared__ uint32_t s_q[PA_P0_WARPS][PA_P0_QMAX];  // queued pairs: lane | site << 5 | slot << 10
+    __shared__ uint32_t s_hit[PA_P0_WARPS];            // lanes whose insertion overlaps
+    __shared__ float s_A[PA_P0_WARPS][18];             // the group's cell, then its inverse
+    typedef St<float> S;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int64_t x = (int64_t(blockIdx.x) * PA_P0_WARPS + wp) * 32 + lane;
+    if ((x - lane) >= ca.n_act) return;  // warp-uniform
+    const bool valid = x < ca.n_act;
+    const int64_t t = valid ? order[x] : 0;
+    const int32_t s = valid ? find_system(ca.sys_off, b.nsys, ca.i_lo + t) : -1;
+    const int32_t fw = valid ? b.framework_of[s] : 0;
+    float rp[3] = {0.f, 0.f, 0.f}, qt[4] = {0.f, 0.f, 0.f, 1.f};
+    if (valid) {
+        const float4 pa = w.pose_a[t], pq = w.pose_b[t];
+        rp[0] = pa.x; rp[1] = pa.y; rp[2] = pa.z;
+        qt[0] = pq.x; qt[1] = pq.y; qt[2] = pq.z; qt[3] = pq.w;
+    }
+    bool hit = false;
+    const float* rho2max = static_cast<const float*>(ca.rho2max);
+    // the guest's radius: the largest body-frame site distance from its reference point
+    float rg = 0.f;
+#pragma unroll
+    for (int a = 0; a < NS; ++a)
+        rg = fmaxf(rg, sqrtf(b.gsite[3 * a] * b.gsite[3 * a] + b.gsite[3 * a + 1] * b.gsite[3 * a + 1] +
+                             b.gsite[3 * a + 2] * b.gsite[3 * a + 2]));
+    unsigned pending = ca.reject ? __ballot_sync(FULL, valid) : 0u;
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const int32_t s0 = __shfl_sync(FULL, s, leader);
+        const bool mine = valid && s == s0;
+        pending &= ~__ballot_sync(FULL, mine);
+        const int32_t f0 = b.framework_of[s0];
+        const int32_t n[3] = {b.ncells[3 * f0], b.ncells[3 * f0 + 1], b.ncells[3 * f0 + 2]};
+        const int32_t m[3] = {reach0[3 * s0], reach0[3 * s0 + 1], reach0[3 * s0 + 2]};
+        bool wide = rho2max == nullptr || 2 * m[0] + 1 >= n[0] || 2 * m[1] + 1 >= n[1] || 2 * m[2] + 1 >= n[2] ||
+                    n[0] >= 1024 || n[1] >= 1024 || n[2] >= 1024;
+        const float* A = b.cells + 9 * f0;
+        const float* iA = b.invcells + 9 * f0;
+        if (lane < 18) s_A[wp][lane] = lane < 9 ? A[lane] : iA[lane - 9];
+        if (lane == 0) s_hit[wp] = 0u;
+        __syncwarp();
+        const float* sA = s_A[wp];
+        const float* siA = s_A[wp] + 9;
+        // the sites in the frame of their home cell moved next to the leader's: e = b + A k with
+        // b = sp - A floor(f); the insertion's reference point c in site 0's frame
+        float e[NS][3], lim[NS], c[3], rc2;
+        int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+        bool off = false;  // sites of one insertion in different frames
+        {
+            int32_t H[3] = {0, 0, 0};
+            float pos[3];
+            matvec_s(sA, rp, pos);
+            float limmax = 0.f;
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                lim[a] = (mine && !wide) ? rho2max[int64_t(s0) * NS + a] + 1e-3f : -1.0f;
+                limmax = fmaxf(limmax, lim[a]);
+            }
+            // the cells an atom within reach of a site can occupy: |df_r| <= d |row r of A^-1|,
+            // d the largest pre-test radius, widened far beyond rounding
+            const float dreach = sqrtf(limmax) + 1e-2f;
+            float dl[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                dl[r] = dreach * float(n[r]) * sqrtf(siA[r] * siA[r] + siA[r + 3] * siA[r + 3] + siA[r + 6] * siA[r + 6]) + 1e-3f;
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                float g[3], sp[3], f[3], fl[3];
+                int32_t h[3], k[3];
+                rotate_s(qt, b.gsite + 3 * a, g);
+                sp[0] = S::add(pos[0], g[0]); sp[1] = S::add(pos[1], g[1]); sp[2] = S::add(pos[2], g[2]);
+                matvec_s(siA, sp, f);
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    h[r] = home_cell_s(wrap_frac_s(f[r]), n[r]);
+                    fl[r] = floorf(f[r]);
+                }
+                if (a == 0) {
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) H[r] = __shfl_sync(FULL, h[r], leader);
+                }
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const int32_t d = H[r] - h[r];
+                    k[r] = 2 * d > n[r] ? 1 : (2 * d < -n[r] ? -1 : 0);
+                    if (mine) {
+                        // the site's reach in cells of the moved frame, inside its own stencil
+                        const float u = (f[r] - fl[r] + float(k[r])) * float(n[r]);
+                        const int32_t hm = h[r] + k[r] * n[r];
+                        lo[r] = min(lo[r], max(int32_t(floorf(u - dl[r])), hm - m[r]));
+                        hi[r] = max(hi[r], min(int32_t(floorf(u + dl[r])), hm + m[r]));
+                    }
+                }
+                const float sx = fl[0] - float(k[0]), sy = fl[1] - float(k[1]), sz = fl[2] - float(k[2]);
+                e[a][0] = sp[0] - (sA[0] * sx + sA[3] * sy + sA[6] * sz);
+                e[a][1] = sp[1] - (sA[1] * sx + sA[4] * sy + sA[7] * sz);
+                e[a][2] = sp[2] - (sA[2] * sx + sA[5] * sy + sA[8] * sz);
+                if (a == 0) { c[0] = e[0][0] - g[0]; c[1] = e[0][1] - g[1]; c[2] = e[0][2] - g[2]; }
+                const float ox = e[a][0] - g[0] - c[0], oy = e[a][1] - g[1] - c[1], oz = e[a][2] - g[2] - c[2];
+                off = off || !(ox * ox + oy * oy + oz * oz < 1e-4f);
+            }
+            const float rr = rg + sqrtf(limmax) + 1e-2f;
+            rc2 = (mine && !wide) ? rr * rr : -1.0f;
+        }
+        wide = wide || __any_sync(FULL, mine && off);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            lo[r] = __reduce_min_sync(FULL, lo[r]);
+            hi[r] = __reduce_max_sync(FULL, hi[r]);
+            wide = wide || hi[r] - lo[r] + 1 > n[r];
+        }
+        if (wide) {  // warp-uniform: the per-site stencil walk
+            if (mine) hit = hardcore_scan<float, NS>(b, s0, f0, rp, qt, rho2, reach0, rho2max);
+            __syncwarp();
+            continue;
+        }
+        const int32_t a0 = b.atom_offsets[f0];
+        const int32_t* coff = b.cell_offsets + b.cellgrid_offsets[f0];
+        const int32_t nt = b.ntypes;
+        const int32_t E0 = hi[0] - lo[0] + 1, E1 = hi[1] - lo[1] + 1;
+        const int32_t ncell = E0 * E1 * (hi[2] - lo[2] + 1);
+        // decide the queued pairs, one lane each
+        const auto flush = [&](int32_t qn) {
+            __syncwarp();
+            for (int32_t q0 = 0; q0 < qn; q0 += 32) {
+                const int32_t qi = q0 + lane;
+                const uint32_t ent = qi < qn ? s_q[wp][qi] : 0u;
+                const int owner = int(ent & 31u), a = int((ent >> 5) & 31u), slot = int((ent >> 10) & 31u);
+                float orp[3], oqt[4];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) orp[r] = __shfl_sync(FULL, rp[r], owner);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) oqt[r] = __shfl_sync(FULL, qt[r], owner);
+                if (qi < qn) {
+                    const float4 at = s_org[wp][slot];
+                    const uint32_t cp = __float_as_uint(s_img[wp][slot].w);
+                    const float r2lim = rho2[(int64_t(s0) * NS + a) * nt + __float_as_int(at.w)];
+                    float pos[3], g[3], sp[3], f[3];
+                    matvec_s(sA, orp, pos);
+                    rotate_s(oqt, b.gsite + 3 * a, g);
+                    sp[0] = S::add(pos[0], g[0]); sp[1] = S::add(pos[1], g[1]); sp[2] = S::add(pos[2], g[2]);
+                    float D[3] = {S::sub(sp[0], at.x), S::sub(sp[1], at.y), S::sub(sp[2], at.z)};
+                    minimum_image_s(sA, siA, D);
+                    const float r2 = dot3s(D[0], D[1], D[2], D[0], D[1], D[2]);
+                    matvec_s(siA, sp, f);
+                    const int32_t cc[3] = {int32_t(cp & 1023u), int32_t((cp >> 10) & 1023u), int32_t(cp >> 20)};
+                    bool in = r2 < r2lim;
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        const int32_t h = home_cell_s(wrap_frac_s(f[r]), n[r]);
+                        int32_t dd = (cc[r] - (h - m[r])) % n[r];
+                        if (dd < 0) dd += n[r];
+                        in = in && dd <= 2 * m[r];
+                    }
+                    if (in) atomicOr(&s_hit[wp], 1u << owner);
+                }
+            }
+            __syncwarp();
+            if ((s_hit[wp] >> lane) & 1u) {
+                hit = true;
+                rc2 = -1.0f;
+#pragma unroll
+                for (int a = 0; a < NS; ++a) lim[a] = -1.0f;
+            }
+        };
+        for (int32_t p0 = 0; p0 < ncell; p0 += 32) {
+            // this round's region cells, one per lane: atom range, image shift, packed cell
+            const int32_t pi = p0 + lane;
+            int32_t j0 = 0, cnt = 0;
+            float Wx = 0.f, Wy = 0.f, Wz = 0.f;
+            uint32_t cpk = 0u;
+            if (pi < ncell) {
+                const int32_t u[3] = {lo[0] + pi % E0, lo[1] + (pi / E0) % E1, lo[2] + pi / (E0 * E1)};
+                int32_t cc[3];
+                float wv[3];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const int32_t wr = floor_div(u[r], n[r]);
+                    cc[r] = u[r] - wr * n[r];
+                    wv[r] = float(wr);
+                }
+                const int32_t ci = cc[0] + n[0] * (cc[1] + n[1] * cc[2]);
+                j0 = a0 + coff[ci];
+                cnt = a0 + coff[ci + 1] - j0;
+                Wx = sA[0] * wv[0] + sA[3] * wv[1] + sA[6] * wv[2];
+                Wy = sA[1] * wv[0] + sA[4] * wv[1] + sA[7] * wv[2];
+                Wz = sA[2] * wv[0] + sA[5] * wv[1] + sA[8] * wv[2];
+                cpk = uint32_t(cc[0]) | (uint32_t(cc[1]) << 10) | (uint32_t(cc[2]) << 20);
+            }
+            int32_t incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int32_t excl = incl - cnt;
+            const int32_t total = __shfl_sync(FULL, incl, 31);
+            for (int32_t q = 0; q < total; q += 32) {
+                // the cell holding staged atom q + lane: the last one starting at or before it
+                const int32_t gi = q + lane;
+                int32_t src = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int32_t ex = __shfl_sync(FULL, excl, src + step);
+                    if (ex <= gi) src += step;
+                }
+                const int32_t js = __shfl_sync(FULL, j0, src) + gi - __shfl_sync(FULL, excl, src);
+                const float sx = __shfl_sync(FULL, Wx, src), sy = __shfl_sync(FULL, Wy, src),
+                            sz = __shfl_sync(FULL, Wz, src);
+                const uint32_t scp = __shfl_sync(FULL, cpk, src);
+                if (gi < total) {
+                    const float4 at = b.atoms[js];
+                    const int32_t ty = b.types[js];
+                    s_img[wp][lane] = make_float4(at.x + sx, at.y + sy, at.z + sz, __uint_as_float(scp));
+                    s_org[wp][lane] = make_float4(at.x, at.y, at.z, __int_as_float(ty));
+                }
+                __syncwarp();
+                const int32_t nb = min(32, total - q);
+                int32_t qn = 0;  // queued pairs (the same on every lane)
+                for (int32_t kk = 0; kk < nb; ++kk) {
+                    const float4 v = s_img[wp][kk];
+                    const float cx = c[0] - v.x, cy = c[1] - v.y, cz = c[2] - v.z;
+                    const bool near = cx * cx + cy * cy + cz * cz < rc2;
+                    if (!__any_sync(FULL, near)) continue;
+#pragma unroll
+                    for (int a = 0; a < NS; ++a) {
+                        const float dx = e[a][0] - v.x, dy = e[a][1] - v.y, dz = e[a][2] - v.z;
+                        const bool cand = near && dx * dx + dy * dy + dz * dz < lim[a];
+                        const uint32_t bal = __ballot_sync(FULL, cand);
+                        if (bal == 0u) continue;
+                        if (qn + __popc(bal) > PA_P0_QMAX) {
+                            flush(qn);
+                            qn = 0;
+                        }
+                        if (cand) s_q[wp][qn + __popc(bal & ((1u << lane) - 1u))] = uint32_t(lane) | (uint32_t(a) << 5) | (uint32_t(kk) << 10);
+                        qn += __popc(bal);
+                    }
+                }
+                if (qn > 0) flush(qn);
+                __syncwarp();  // the staged batch is no longer read
+            }
+        }
+    }
+    if (!valid) return;
+    if (hit) {
         mark_rejected(w, t, NS);
         return;
     }
