@@ -92,36 +92,62 @@ def build_rejection_tables(batch, kT):
 def _reduce(sW, sUW, n, kT, V, s):
     """Block means, delta-method errors -> WidomResult; throws on non-finite sums or mu_ex/q_st
     (src/widom.jl:451-492). s is the 1-based system index used in messages."""
-    sW = np.asarray(sW, dtype=np.float64)
-    sUW = np.asarray(sUW, dtype=np.float64)
-    n = np.asarray(n)
-    nb = len(sW)
-    if not np.all(n > 0):
-        raise ArgumentError(f"block {int(np.argmin(n > 0)) + 1} of {nb} has zero samples")
-    kT64, V64 = float(kT), float(V)
-    mW = sW / n
-    mUW = sUW / n
-    W = float(np.sum(sW)) / float(np.sum(n))
-    UW = float(np.sum(sUW)) / float(np.sum(n))
-    if not (math.isfinite(W) and math.isfinite(UW)):
-        raise ArgumentError(f"system {s}: Boltzmann accumulation overflowed Float64 (W={W}, UW={UW}); an "
-                            "insertion energy below about -709·kT was sampled")
-    varW = float(np.sum((mW - W) ** 2)) / (nb - 1)
-    varUW = float(np.sum((mUW - UW) ** 2)) / (nb - 1)
-    cov = float(np.sum((mW - W) * (mUW - UW))) / (nb - 1)
-    semW = math.sqrt(varW / nb)
+    return _reduce_rows(np.asarray(sW, dtype=np.float64)[None, :], np.asarray(sUW, dtype=np.float64)[None, :],
+                        np.asarray(n)[None, :], kT, np.array([float(V)]), first=s)[0]
+
+
+def _div(a, b):
+    """a / b on Python floats with IEEE semantics for b == 0 (inf or nan instead of an exception)."""
+    if b != 0:
+        return a / b
+    if a == 0 or math.isnan(a):
+        return math.nan
+    return math.copysign(math.inf, a) * math.copysign(1.0, b)
+
+
+def _reduce_rows(sW, sUW, n, kT, V, first=1):
+    """_reduce for every row (system) of the nsys x nblocks block sums at once: the block
+    statistics as array operations over all systems, then the checks and the result of each
+    system in order (the first failing system raises, as a loop of _reduce would)."""
+    nsys, nb = sW.shape
+    kT64 = float(kT)
+    ntot = n.sum(axis=1)
     with np.errstate(all="ignore"):
-        ratio = UW / W if W != 0 else (math.nan if UW == 0 else math.copysign(math.inf, UW))
-        var_ratio = 0.0 if UW == 0 else ratio**2 * (varUW / UW**2 + varW / W**2 - 2 * cov / (UW * W)) / nb
-        mu_ex = -kT64 * math.log(W) if W > 0 else math.inf
-    q_st = kT64 - ratio
-    for name, v in (("mu_ex", mu_ex), ("q_st", q_st)):
-        if not math.isfinite(v):
-            raise ArgumentError(f"system {s}: {name} = {v} is not finite")
-    with np.errstate(all="ignore"):
-        mu_err = kT64 * semW / W if W != 0 else math.inf
-    return WidomResult(mu_ex, mu_err, V64 * W / kT64, V64 * semW / kT64, q_st,
-                       math.sqrt(max(var_ratio, 0.0)) if not math.isnan(var_ratio) else math.nan, int(np.sum(n)), nb)
+        mW = sW / n
+        mUW = sUW / n
+        W = sW.sum(axis=1) / ntot
+        UW = sUW.sum(axis=1) / ntot
+        dW = mW - W[:, None]
+        dUW = mUW - UW[:, None]
+        varW = (dW * dW).sum(axis=1) / (nb - 1)
+        varUW = (dUW * dUW).sum(axis=1) / (nb - 1)
+        cov = (dW * dUW).sum(axis=1) / (nb - 1)
+        semW = np.sqrt(varW / nb)
+    empty = (n <= 0).any(axis=1).tolist()
+    W, UW, varW, varUW, cov, semW = W.tolist(), UW.tolist(), varW.tolist(), varUW.tolist(), cov.tolist(), semW.tolist()
+    ntot, V = ntot.tolist(), np.asarray(V, dtype=np.float64).tolist()
+    out = []
+    for r in range(nsys):
+        s = first + r
+        if empty[r]:
+            raise ArgumentError(f"block {int(np.argmin(n[r] > 0)) + 1} of {nb} has zero samples")
+        w, uw = W[r], UW[r]
+        if not (math.isfinite(w) and math.isfinite(uw)):
+            raise ArgumentError(f"system {s}: Boltzmann accumulation overflowed Float64 (W={w}, UW={uw}); an "
+                                "insertion energy below about -709·kT was sampled")
+        ratio = uw / w if w != 0 else (math.nan if uw == 0 else math.copysign(math.inf, uw))
+        var_ratio = 0.0 if uw == 0 else ratio * ratio * (_div(varUW[r], uw * uw) + _div(varW[r], w * w) -
+                                                          2 * _div(cov[r], uw * w)) / nb
+        mu_ex = -kT64 * math.log(w) if w > 0 else math.inf
+        q_st = kT64 - ratio
+        for name, v in (("mu_ex", mu_ex), ("q_st", q_st)):
+            if not math.isfinite(v):
+                raise ArgumentError(f"system {s}: {name} = {v} is not finite")
+        mu_err = kT64 * semW[r] / w if w != 0 else math.inf
+        out.append(WidomResult(mu_ex, mu_err, V[r] * w / kT64, V[r] * semW[r] / kT64, q_st,
+                               math.sqrt(max(var_ratio, 0.0)) if not math.isnan(var_ratio) else math.nan,
+                               int(ntot[r]), nb))
+    return out
 
 
 class B200Backend:
@@ -225,8 +251,9 @@ def _widom(batch, guest, *, reject, T, ninsert, backend=None, seed=0, chunk=2**1
 
 def block_sums(lse, sw, suw):
     """Σ W and Σ dU W per block from the library's (max, scaled sums) representation."""
+    neg = np.isneginf(lse)
     with np.errstate(over="ignore", invalid="ignore"):
-        scale = np.where(np.isneginf(lse), 0.0, np.exp(np.where(np.isneginf(lse), 0.0, lse)))
+        scale = np.exp(lse) if not neg.any() else np.where(neg, 0.0, np.exp(np.where(neg, 0.0, lse)))
         return scale * sw, scale * suw
 
 
@@ -242,11 +269,9 @@ def lnkh_from_sums(batch, kT, nblocks, lse, sw, suw, cnt):
 
 def _results(batch, kT, nblocks, lse, sw, suw, cnt):
     sW, sUW = block_sums(lse, sw, suw)
-    sW = sW.reshape(batch.nsys, nblocks)
-    sUW = sUW.reshape(batch.nsys, nblocks)
-    cnt = cnt.reshape(batch.nsys, nblocks)
-    Vf = batch.volumes.astype(batch.T).astype(np.float64)
-    return [_reduce(sW[s], sUW[s], cnt[s], kT, Vf[int(batch.framework_of[s]) - 1], s + 1) for s in range(batch.nsys)]
+    Vf = batch.volumes.astype(batch.T).astype(np.float64)[np.asarray(batch.framework_of, dtype=np.int64) - 1]
+    return _reduce_rows(sW.reshape(batch.nsys, nblocks), sUW.reshape(batch.nsys, nblocks),
+                        np.asarray(cnt).reshape(batch.nsys, nblocks), kT, Vf)
 
 
 def widom(batch, guest, *, T, ninsert, backend=None, seed=0, chunk=2**16, nblocks=10, run=None):
