@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
         const float NLOG2E = -1.4426950408889634f;
         const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
+        const float halpha = 0.5f * alpha;
         float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
         // LJ parameters of the current host type for this lane's site: list entries come in runs of
         // one type (the bin's run table), the same for every lane, so the loop runs uniformly from
@@ -174,8 +175,8 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                     if (PQ) { sp += u; sq = fmaf(x3, x3, sq + u); }
                                 }
                                 if (EQCUT || r2 < re2) {
-                                    const float z = alpha * (r2 * ri);
-                                    const float tt = rcp_nr(fmaf(0.5f, z, 1.0f));
+                                    // t = 1 / (1 + z/2), z = alpha r, with alpha/2 exact
+                                    const float tt = rcp_nr(fmaf(halpha, r2 * ri, 1.0f));
                                     const float cf[PA_NERFC32] = PA_ERFC32_INIT;
                                     float p = cf[PA_NERFC32 - 1];
 #pragma unroll
