@@ -26,10 +26,10 @@ import __graft_entry__ as ge  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
-# DRAM bytes (read + write) of one k_energy32 launch on this workload with 3.5 Å bins, from an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum); it cannot be measured inside the bench
-ENERGY32_TRAFFIC_BYTES = 69.985792e6 + 8.245248e6
-ENERGY32_TRAFFIC_BIN_WIDTH = 3.5
+# DRAM bytes (read + write) of one k_energy32 launch on this workload, per bin width (the
+# autotuner's choice), from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum); they
+# cannot be measured inside the bench
+ENERGY32_TRAFFIC_BYTES = {3.0: 83.832064e6 + 8.302592e6, 3.5: 70.104320e6 + 7.413248e6}
 # the metric and workload names of both arms (ours and the reference's CPU implementation)
 METRIC = "Widom insertions/s (CO2, 5,832-atom framework)"
 WORKLOAD = "co2_5832_atoms_3x3x3_monoclinic"
@@ -109,9 +109,9 @@ def load_peaks():
 
 
 def fp32_peak(torch):
-    """Measured FP32 FMA throughput of this GPU (TFLOP/s): a large elementwise multiply-add chain
-    kernel is memory bound, so instead time torch.addcmul_ on L2-resident data repeatedly as a
-    lower bound and fall back to the nominal figure when that is below it."""
+    """The FP32 FMA peak the energy kernel's roofline uses (TFLOP/s): the nominal figure at the
+    maximum SM clock. The measured peaks file holds HBM copy bandwidth and bf16 GEMM throughput
+    only, neither of which bounds this FP32 CUDA-core kernel."""
     return FP32_PEAK_NOMINAL
 
 
@@ -474,8 +474,8 @@ def main():
         peak = fp32_peak(torch)
         ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": ENERGY32_TRAFFIC_BYTES if (args.ninsert == 1_000_000 and world == 1
-                                                      and tune.bin_width == ENERGY32_TRAFFIC_BIN_WIDTH) else None,
+                "traffic": ENERGY32_TRAFFIC_BYTES.get(float(tune.bin_width))
+                if (args.ninsert == 1_000_000 and world == 1) else None,
                 "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
                 "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
                 "flops_per_survivor": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
