@@ -83,7 +83,8 @@ struct CallArgs {
     int64_t k_offset;
     const int64_t* koff_dev;
     // optional (F-typed, nsys*N): each (system, site)'s largest rejection radius squared, for
-    // phase 0's relaxed pre-test; NULL: every atom of the stencil takes the strict test
+    // phase 0's relaxed pre-test; NULL: every atom of the stencil takes the strict test (the
+    // FP32 warp kernel then runs the per-site stencil scan)
     const void* rho2max;
 };
 
@@ -334,9 +335,9 @@ __global__ void __launch_bounds__(256, 4) k_pose(DevBatch<F> b, CallArgs ca, Wor
 // ---------------------------------------------------------------------------------------------
 // The FP32 path splits k_pose in two so that phase 0 runs in spatial order: k_draw32 draws every
 // pose and gives it a slot in its centre's sub-bin (a scan and scatter then order all insertions
-// by sub-bin), and k_phase0_32 scans the hard core of the insertions in that order. Neighbouring
-// threads then walk nearly the same cells and mostly reach the same outcome, where insertion
-// order gives every thread an unrelated stencil and exit point.
+// by sub-bin), and k_phase0_32 tests the hard core of the insertions in that order. The 32
+// insertions of a warp then share nearly all of their stencil cells, which the warp stages once,
+// where insertion order gives every lane an unrelated stencil.
 // ---------------------------------------------------------------------------------------------
 template <int NS>
 __global__ void __launch_bounds__(256) k_draw32(DevBatch<float> b, CallArgs ca, Work w, Work wa) {
