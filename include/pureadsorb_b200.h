@@ -116,8 +116,10 @@ typedef struct pa_batch_desc {
 /* Uploads a batch for the given precision (PA_PRECISION_F32 or _F64) and builds the device-side
  * tables the kernels read (per-framework spatial bins with their imaged neighbour lists for the
  * FP32 path). Replaces `adapt(backend, batch)` (src/widom.jl:368). The host arrays may be released
- * on return; the last list-build kernel may still be running on the context's stream, and every
- * later call on the context is ordered after it. */
+ * on return. The neighbour-list fill may still be running on return, on a second stream of the
+ * context, so that it overlaps the next call's pose draw and phase 0: every later call that reads
+ * the lists first orders the context's stream after the context's last fill (pa_widom just before
+ * its energy kernel; an external event node when the stream is being captured). */
 pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t precision, pa_batch** out);
 pa_status pa_batch_free(pa_batch* batch);
 /* Replaces an uploaded batch's LJ pair tables and per-framework constant offsets in place: the

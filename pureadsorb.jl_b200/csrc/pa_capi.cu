@@ -50,6 +50,12 @@ struct pa_context {
     int32_t device = 0;
     int32_t num_sms = 148;
     cudaStream_t own = nullptr, stream = nullptr;
+    // the FP32 upload's neighbour-list fill runs on `aux`, after `up` (recorded on the stream
+    // once the tables are on the device), so that it overlaps the next call's pose draw and phase
+    // 0; `lists` is recorded on `aux` after every fill, and work that reads lists waits for it
+    // (its most recent record: a no-op once the fill is done)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t up = nullptr, lists = nullptr;
     std::string err;
     bool timing = false;
     double ms[NCLASS] = {0};
@@ -121,6 +127,7 @@ struct pa_batch {
     const double* q64 = nullptr;       // FP64 charges of the stored atoms (inside the arena)
     const int32_t* types0 = nullptr;   // 0-based types (inside the arena)
     // cudaFree returns stream-ordered pool memory synchronously, so the next upload reuses it
+    // (it also waits for every stream, a fill in flight included)
     ~pa_batch() {
         if (arena) cudaFree(arena);
         if (lists) cudaFree(lists);
@@ -254,15 +261,15 @@ std::vector<Seg> segments(const std::vector<int64_t>& ns, const std::vector<int6
 }
 
 struct Timer {
-    pa_context* ctx; int cls; cudaEvent_t a = nullptr, b = nullptr;
-    Timer(pa_context* c, int k) : ctx(c), cls(k) {
+    pa_context* ctx; int cls; cudaStream_t st; cudaEvent_t a = nullptr, b = nullptr;
+    Timer(pa_context* c, int k, cudaStream_t s = nullptr) : ctx(c), cls(k), st(s ? s : c->stream) {
         if (!ctx->timing) return;
         cudaEventCreate(&a); cudaEventCreate(&b);
-        cudaEventRecord(a, ctx->stream);
+        cudaEventRecord(a, st);
     }
     void stop(int nlaunch) {
         if (!ctx->timing) return;
-        cudaEventRecord(b, ctx->stream);
+        cudaEventRecord(b, st);
         ctx->pending.push_back({cls, nlaunch, a, b});
         a = b = nullptr;
     }
@@ -280,6 +287,16 @@ template <typename F> pa::DevBatch<F>& view(pa_batch* B);
 template <> pa::DevBatch<float>& view<float>(pa_batch* B) { return B->d32; }
 template <> pa::DevBatch<double>& view<double>(pa_batch* B) { return B->d64; }
 template <typename F> const pa::DevBatch<F>& cview(const pa_batch* B) { return view<F>(const_cast<pa_batch*>(B)); }
+
+// Orders the context's stream after the last neighbour-list fill of the context (as an
+// external event node when the stream is being captured).
+pa_status lists_wait(pa_context* ctx) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PA_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    const unsigned flags = cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : cudaEventWaitDefault;
+    PA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->lists, flags));
+    return PA_OK;
+}
 
 pa_status wait_stream(pa_context* ctx) {
     auto t0 = std::chrono::steady_clock::now();
@@ -560,17 +577,22 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         g.type_out = reinterpret_cast<int32_t*>(lb + o.list_type);
         g.atom_out = reinterpret_cast<int32_t*>(lb + o.list_atom);
         if (B->nbins > 0) {
-            Timer tm(ctx, 4);
-            pa::k_lists<true><<<B->nbins, 256, 0, st>>>(g);
-            pa::k_runs<<<B->nbins, 32, 0, st>>>(g.offsets, g.type_out, reinterpret_cast<int2*>(lb + o.list_runs),
-                                                B->runs_per_bin);
+            // the fill on the aux stream, after everything above; later work that reads the
+            // lists waits for ctx->lists (lists_wait; pa_widom just before the energy kernel)
+            PA_CUDA(ctx, cudaEventRecord(ctx->up, st));
+            PA_CUDA(ctx, cudaStreamWaitEvent(ctx->aux, ctx->up, 0));
+            Timer tm(ctx, 4, ctx->aux);
+            pa::k_lists<true><<<B->nbins, 256, 0, ctx->aux>>>(g);
+            pa::k_runs<<<B->nbins, 32, 0, ctx->aux>>>(g.offsets, g.type_out, reinterpret_cast<int2*>(lb + o.list_runs),
+                                                      B->runs_per_bin);
             tm.stop(2);
             PA_CUDA(ctx, cudaGetLastError());
+            PA_CUDA(ctx, cudaEventRecord(ctx->lists, ctx->aux));
         }
     }
     fill_batch_view(B, view<F>(B), desc, o);
-    // the fill pass is stream-ordered before every later use of the batch on this context, so the
-    // host does not wait for it (its errors surface at the next wait, like any kernel's)
+    // the host does not wait for the fill pass (its errors surface at the next wait, like any
+    // kernel's)
     return lists ? PA_OK : wait_stream(ctx);
 }
 
@@ -698,6 +720,15 @@ pa_status pa_context_create(int32_t device, pa_context** out) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->up, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->lists, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(ctx->own);
+        if (ctx->aux) cudaStreamDestroy(ctx->aux);
+        if (ctx->up) cudaEventDestroy(ctx->up);
+        delete ctx;
+        return PA_ERR_CUDA;
+    }
     ctx->stream = ctx->own;
     *out = ctx;
     return PA_OK;
@@ -707,7 +738,11 @@ pa_status pa_context_destroy(pa_context* ctx) {
     if (!ctx) return PA_ERR_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->aux);
     if (ctx->own) cudaStreamDestroy(ctx->own);
+    if (ctx->aux) cudaStreamDestroy(ctx->aux);
+    if (ctx->up) cudaEventDestroy(ctx->up);
+    if (ctx->lists) cudaEventDestroy(ctx->lists);
     delete ctx;
     return PA_OK;
 }
@@ -824,6 +859,7 @@ pa_status pa_batch_set_pair_tables(pa_context* ctx, pa_batch* B, const double* s
     if (!ctx || !B || !sigma || !epsilon || !constant_offset) return fail(ctx, PA_ERR_ARG, "null argument");
     if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    if (pa_status lw = lists_wait(ctx); lw != PA_OK) return lw;
     return B->precision == PA_PRECISION_F32 ? set_pair_tables_impl<float>(ctx, B, sigma, epsilon, constant_offset)
                                             : set_pair_tables_impl<double>(ctx, B, sigma, epsilon, constant_offset);
 }
@@ -832,6 +868,7 @@ pa_status pa_batch_hardcore_bounds(pa_context* ctx, const pa_batch* B, double* b
     if (!ctx || !B || !bs) return fail(ctx, PA_ERR_ARG, "null argument");
     if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    if (pa_status lw = lists_wait(ctx); lw != PA_OK) return lw;
     const int N = B->nguest, nt = B->ntypes, nfw = B->nfw;
     // [site sigma N*nt][site eps N*nt][guest charges N][error flag][chunk sums nfw*nchunk]
     int64_t amax = 0;
@@ -1127,6 +1164,12 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
             }
             tm.stop(2);
             PA_CUDA(ctx, cudaGetLastError());
+        }
+        // a neighbour-list fill still in flight from the upload (an external event node in the
+        // call's graph)
+        if (f32) {
+            pa_status lw = lists_wait(ctx);
+            if (lw != PA_OK) return lw;
         }
         {
             Timer tm(ctx, 2);
@@ -1561,6 +1604,7 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     if (per && (per->flags || per->poses))
         return fail(ctx, PA_ERR_ARG, "pa_widom_static returns per-insertion dU only (flags and poses need host staging)");
     if (args->chain) return fail(ctx, PA_ERR_ARG, "pa_widom_static does not take a loaded configuration");
+    if (pa_status lw = lists_wait(ctx); lw != PA_OK) return lw;
     const int64_t ninsert = args->ninsert, nblocks = args->nblocks, run = args->run;
     if (ninsert < 1 || nblocks < 1 || run < 1) return fail(ctx, PA_ERR_ARG, "ninsert, nblocks and run must be >= 1");
     if (!(std::isfinite(args->kT) && args->kT != 0)) return fail(ctx, PA_ERR_ARG, "kT must be finite and nonzero");
