@@ -56,6 +56,8 @@ struct pa_context {
     // (its most recent record: a no-op once the fill is done)
     cudaStream_t aux = nullptr;
     cudaEvent_t up = nullptr, lists = nullptr;
+    cudaEvent_t counted = nullptr;  // recorded after the count pass's totals reach h_counts
+    cudaEvent_t staged = nullptr;   // recorded after the last copy out of h_stage
     std::string err;
     bool timing = false;
     double ms[NCLASS] = {0};
@@ -89,6 +91,10 @@ struct pa_context {
     int32_t* h_cnt = nullptr;
     char* h_stage = nullptr;  // pinned staging of batch uploads
     size_t h_stage_cap = 0;
+    char* h_stage_l = nullptr;  // pinned staging of the list build's inputs (uploaded first)
+    size_t h_stage_l_cap = 0;
+    int32_t* h_counts = nullptr;  // pinned: the count pass's per-bin totals
+    size_t h_counts_cap = 0;
     std::vector<int64_t> up_seg_rng, up_sys_off;
     std::vector<int32_t> up_reach0;
     std::vector<unsigned char> up_rho2;
@@ -98,6 +104,8 @@ struct pa_context {
         if (h_seg) cudaFreeHost(h_seg);
         if (h_cnt) cudaFreeHost(h_cnt);
         if (h_stage) cudaFreeHost(h_stage);
+        if (h_stage_l) cudaFreeHost(h_stage_l);
+        if (h_counts) cudaFreeHost(h_counts);
     }
 };
 
@@ -111,6 +119,7 @@ struct pa_batch {
     // two stream-ordered allocations: the packed static tables, and the neighbour lists
     void* arena = nullptr;
     void* lists = nullptr;
+    void* arena_l = nullptr;  // FP32: the list build's inputs (bins, FP32 fractional coordinates, ...)
     pa::DevBatch<float> d32{};
     pa::DevBatch<double> d64{};
     // for the adjoint: FP64 fractional coordinates of the stored atoms (FP32 batches), 2 kpref per
@@ -131,6 +140,7 @@ struct pa_batch {
     ~pa_batch() {
         if (arena) cudaFree(arena);
         if (lists) cudaFree(lists);
+        if (arena_l) cudaFree(arena_l);
     }
 };
 
@@ -175,25 +185,26 @@ cudaError_t upload_cached(DevMem& m, std::vector<T>& cache, const std::vector<T>
 // of it has always finished (every upload waits on its stream before its list fill pass or its
 // return, and a failed upload synchronises).
 struct Packer {
-    pa_context* ctx;
+    char*& buf;    // a grow-only pinned staging buffer of the context
+    size_t& cap;
     size_t n = 0;
     bool ok = true;
-    explicit Packer(pa_context* c) : ctx(c) {}
+    Packer(char*& b, size_t& c) : buf(b), cap(c) {}
     bool grow(size_t need) {
-        if (need <= ctx->h_stage_cap) return true;
-        const size_t cap = std::max(need, std::max(2 * ctx->h_stage_cap, size_t(1) << 20));
+        if (need <= cap) return true;
+        const size_t nc = std::max(need, std::max(2 * cap, size_t(1) << 20));
         char* p = nullptr;
-        if (cudaMallocHost(reinterpret_cast<void**>(&p), cap) != cudaSuccess) { ok = false; return false; }
-        if (n) std::memcpy(p, ctx->h_stage, n);
-        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
-        ctx->h_stage = p;
-        ctx->h_stage_cap = cap;
+        if (cudaMallocHost(reinterpret_cast<void**>(&p), nc) != cudaSuccess) { ok = false; return false; }
+        if (n) std::memcpy(p, buf, n);
+        if (buf) cudaFreeHost(buf);
+        buf = p;
+        cap = nc;
         return true;
     }
     template <typename T> size_t add(const std::vector<T>& v) {
         const size_t off = (n + 255) & ~size_t(255), bytes = std::max<size_t>(v.size() * sizeof(T), 16);
         if (!grow(off + bytes)) return 0;
-        if (!v.empty()) std::memcpy(ctx->h_stage + off, v.data(), v.size() * sizeof(T));
+        if (!v.empty()) std::memcpy(buf + off, v.data(), v.size() * sizeof(T));
         n = off + bytes;
         return off;
     }
@@ -201,7 +212,7 @@ struct Packer {
         const size_t off = (n + 255) & ~size_t(255);
         bytes = std::max<size_t>(bytes, 16);
         if (!grow(off + bytes)) return 0;
-        std::memset(ctx->h_stage + off, 0, bytes);
+        std::memset(buf + off, 0, bytes);
         n = off + bytes;
         return off;
     }
@@ -298,6 +309,21 @@ pa_status lists_wait(pa_context* ctx) {
     return PA_OK;
 }
 
+// Waits on the host for an event (polling, bounded like wait_stream); an event never recorded
+// counts as done.
+pa_status wait_event(pa_context* ctx, cudaEvent_t ev) {
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return PA_OK;
+        if (e != cudaErrorNotReady) return fail(ctx, PA_ERR_CUDA, std::string("device work failed: ") + cudaGetErrorString(e));
+        double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (dt > WAIT_LIMIT_S) return fail(ctx, PA_ERR_TIMEOUT, "device work did not finish within the host wait limit");
+        if (dt < 0.05) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(500));
+    }
+}
+
 pa_status wait_stream(pa_context* ctx) {
     auto t0 = std::chrono::steady_clock::now();
     for (;;) {
@@ -366,6 +392,110 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     cudaStream_t st = ctx->stream;
     const int nfw = desc->nfw, N = desc->nguest, nt = desc->ntypes;
     const int64_t na = B->natoms, nk = B->nk;
+    // spatial bins
+    std::vector<int32_t> bdims(3 * nfw), bbase(nfw + 1, 0), bfw;
+    std::vector<double> radius2(nfw);
+    std::vector<int32_t> nimg(nfw);
+    std::vector<float> reach(3 * nfw);
+    const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
+    double binw = ctx->tuning.bin_width > 0 ? ctx->tuning.bin_width : DEFAULT_BIN_WIDTH;
+    for (int fw = 0; fw < nfw; ++fw) {
+        double L[3];
+        perpendicular_lengths(desc->cells + 9 * fw, L);
+        for (int r = 0; r < 3; ++r)
+            bdims[3 * fw + r] = (sizeof(F) == 4) ? std::max(1, int(std::floor(L[r] / binw))) : 1;
+        bbase[fw + 1] = bbase[fw] + bdims[3 * fw] * bdims[3 * fw + 1] * bdims[3 * fw + 2];
+        for (int32_t q = bbase[fw]; q < bbase[fw + 1]; ++q) bfw.push_back(fw);
+        // circumradius of one bin: half the longest body diagonal
+        const double* A = desc->cells + 9 * fw;
+        double circ = 0;
+        for (int sx = -1; sx <= 1; sx += 2)
+            for (int sy = -1; sy <= 1; sy += 2) {
+                double d[3] = {sx / double(bdims[3 * fw]), sy / double(bdims[3 * fw + 1]), 1.0 / bdims[3 * fw + 2]};
+                double v[3];
+                for (int r = 0; r < 3; ++r) v[r] = A[r] * d[0] + A[r + 3] * d[1] + A[r + 6] * d[2];
+                circ = std::max(circ, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+            }
+        // every FP32 work item is one guest site, binned by the site's own position: its pairs
+        // lie within rc of a point of its bin
+        double R = rcmax + circ + 1.0e-3;
+        radius2[fw] = R * R;
+        // an image n of a fractional offset d in [-1/2, 1/2]^3 lies within R only if
+        // |d_r + n_r| <= R / L_r on every axis, so |n_r| <= floor(R / L_r + 1/2)
+        double Lmin = std::min(L[0], std::min(L[1], L[2]));
+        nimg[fw] = int32_t(std::floor(R / Lmin + 0.5));
+        // the per-axis image bound of the list build, widened far beyond FP32 rounding
+        for (int r = 0; r < 3; ++r) reach[3 * fw + r] = float(R / L[r] * (1.0 + 1.0e-6) + 1.0e-5);
+    }
+    B->nbins = bbase[nfw];
+    // FP32: the neighbour-list count pass goes first. Its inputs (bins, the atoms' FP32 fractional
+    // coordinates in type-major order, the per-framework reach) are staged and uploaded on their
+    // own and the pass is launched before the rest of the tables are prepared, so that the host
+    // work below overlaps the copy and the pass.
+    const bool lists = sizeof(F) == 4;
+    std::vector<double> frac;
+    std::vector<int32_t> order;
+    pa::ListGeom g{};
+    if (lists) {
+        frac.resize(3 * na);
+        for (int fw = 0; fw < nfw; ++fw) {
+            const double* iA = desc->invcells + 9 * fw;
+            for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
+                for (int r = 0; r < 3; ++r)
+                    frac[3 * j + r] = iA[r] * desc->positions[3 * j] + iA[r + 3] * desc->positions[3 * j + 1] +
+                                      iA[r + 6] * desc->positions[3 * j + 2];
+        }
+        // each framework's atoms in type-major order (a stable counting sort): list entries of one
+        // type form one run; beside it the FP32 fractional coordinates in that order, which the
+        // list build's membership test reads coalesced
+        order.resize(na);
+        std::vector<int32_t> tstart(nt + 1);
+        std::vector<float4> fr32(na);
+        for (int fw = 0; fw < nfw; ++fw) {
+            const int32_t a0 = B->atom_offsets[fw], a1 = B->atom_offsets[fw + 1];
+            std::fill(tstart.begin(), tstart.end(), 0);
+            for (int32_t j = a0; j < a1; ++j) ++tstart[desc->types[j]];
+            for (int t = 0; t < nt; ++t) tstart[t + 1] += tstart[t];
+            for (int32_t j = a0; j < a1; ++j) order[a0 + tstart[desc->types[j] - 1]++] = j;
+            for (int32_t rk = a0; rk < a1; ++rk) {
+                const int32_t j = order[rk];
+                fr32[rk] = make_float4(float(frac[3 * j]), float(frac[3 * j + 1]), float(frac[3 * j + 2]), 0.f);
+            }
+        }
+        Packer pl(ctx->h_stage_l, ctx->h_stage_l_cap);
+        const size_t l_dims = pl.add(bdims), l_base = pl.add(bbase), l_fw = pl.add(bfw), l_aoff = pl.add(B->atom_offsets);
+        const size_t l_fr32 = pl.add(fr32), l_cells = pl.add(std::vector<double>(desc->cells, desc->cells + 9 * nfw));
+        const size_t l_r2 = pl.add(radius2), l_nimg = pl.add(nimg), l_reach = pl.add(reach);
+        const size_t l_count = pl.reserve(sizeof(int32_t) * std::max(1, B->nbins));
+        if (!pl.ok) return fail(ctx, PA_ERR_CUDA, "pinned staging allocation failed");
+        if (ctx->h_counts_cap < size_t(std::max(1, B->nbins))) {
+            if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
+            ctx->h_counts = nullptr; ctx->h_counts_cap = 0;
+            PA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_counts), sizeof(int32_t) * std::max(1, B->nbins)));
+            ctx->h_counts_cap = size_t(std::max(1, B->nbins));
+        }
+        PA_CUDA(ctx, cudaMallocAsync(&B->arena_l, pl.n, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(B->arena_l, ctx->h_stage_l, pl.n, cudaMemcpyHostToDevice, st));
+        const char* lb0 = static_cast<const char*>(B->arena_l);
+        g.bin_dims = reinterpret_cast<const int32_t*>(lb0 + l_dims);
+        g.bin_base = reinterpret_cast<const int32_t*>(lb0 + l_base);
+        g.bin_fw = reinterpret_cast<const int32_t*>(lb0 + l_fw);
+        g.atom_offsets = reinterpret_cast<const int32_t*>(lb0 + l_aoff);
+        g.fr32 = reinterpret_cast<const float4*>(lb0 + l_fr32);
+        g.cells = reinterpret_cast<const double*>(lb0 + l_cells);
+        g.radius2 = reinterpret_cast<const double*>(lb0 + l_r2);
+        g.nimg = reinterpret_cast<const int32_t*>(lb0 + l_nimg);
+        g.reach = reinterpret_cast<const float*>(lb0 + l_reach);
+        g.counts = reinterpret_cast<int32_t*>(const_cast<char*>(lb0) + l_count);
+        if (B->nbins > 0) {
+            Timer tm(ctx, 4);
+            pa::k_lists<false><<<B->nbins, 256, 0, st>>>(g);
+            tm.stop(1);
+            PA_CUDA(ctx, cudaGetLastError());
+            PA_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, g.counts, sizeof(int32_t) * B->nbins, cudaMemcpyDeviceToHost, st));
+        }
+        PA_CUDA(ctx, cudaEventRecord(ctx->counted, st));
+    }
     std::vector<int32_t> fwo(desc->nsys);
     for (int s = 0; s < desc->nsys; ++s) fwo[s] = desc->framework_of[s] - 1;
     std::vector<F> cells(9 * nfw), inv(9 * nfw);
@@ -429,44 +559,11 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             B->site_eps[a * nt + t] = e;
         }
     }
-    // spatial bins
-    std::vector<int32_t> bdims(3 * nfw), bbase(nfw + 1, 0), bfw;
-    std::vector<double> radius2(nfw);
-    std::vector<int32_t> nimg(nfw);
-    std::vector<float> reach(3 * nfw);
-    const double rcmax = std::max(desc->cutoff, desc->ewald_cutoff);
-    double binw = ctx->tuning.bin_width > 0 ? ctx->tuning.bin_width : DEFAULT_BIN_WIDTH;
-    for (int fw = 0; fw < nfw; ++fw) {
-        double L[3];
-        perpendicular_lengths(desc->cells + 9 * fw, L);
-        for (int r = 0; r < 3; ++r)
-            bdims[3 * fw + r] = (sizeof(F) == 4) ? std::max(1, int(std::floor(L[r] / binw))) : 1;
-        bbase[fw + 1] = bbase[fw] + bdims[3 * fw] * bdims[3 * fw + 1] * bdims[3 * fw + 2];
-        for (int32_t q = bbase[fw]; q < bbase[fw + 1]; ++q) bfw.push_back(fw);
-        // circumradius of one bin: half the longest body diagonal
-        const double* A = desc->cells + 9 * fw;
-        double circ = 0;
-        for (int sx = -1; sx <= 1; sx += 2)
-            for (int sy = -1; sy <= 1; sy += 2) {
-                double d[3] = {sx / double(bdims[3 * fw]), sy / double(bdims[3 * fw + 1]), 1.0 / bdims[3 * fw + 2]};
-                double v[3];
-                for (int r = 0; r < 3; ++r) v[r] = A[r] * d[0] + A[r + 3] * d[1] + A[r + 6] * d[2];
-                circ = std::max(circ, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
-            }
-        // every FP32 work item is one guest site, binned by the site's own position: its pairs
-        // lie within rc of a point of its bin
-        double R = rcmax + circ + 1.0e-3;
-        radius2[fw] = R * R;
-        // an image n of a fractional offset d in [-1/2, 1/2]^3 lies within R only if
-        // |d_r + n_r| <= R / L_r on every axis, so |n_r| <= floor(R / L_r + 1/2)
-        double Lmin = std::min(L[0], std::min(L[1], L[2]));
-        nimg[fw] = int32_t(std::floor(R / Lmin + 0.5));
-        // the per-axis image bound of the list build, widened far beyond FP32 rounding
-        for (int r = 0; r < 3; ++r) reach[3 * fw + r] = float(R / L[r] * (1.0 + 1.0e-6) + 1.0e-5);
-    }
-    B->nbins = bbase[nfw];
-    // one packed upload of every table (and the list build's temporaries)
-    Packer pk(ctx);
+    // one packed upload of every other table (and of the fill pass's inputs); the staging buffer
+    // is free once the previous upload's copy out of it is done
+    if (pa_status ws = wait_event(ctx, ctx->staged); ws != PA_OK) return ws;
+    Packer pk(ctx->h_stage, ctx->h_stage_cap);
+    size_t t_frac = 0, t_order = 0;
     Slots o{};
     o.framework_of = pk.add(fwo); o.cells = pk.add(cells); o.invcells = pk.add(inv); o.alphas = pk.add(alphas);
     o.const_offset = pk.add(co); o.atom_offsets = pk.add(B->atom_offsets); o.atoms = pk.add(atoms);
@@ -475,42 +572,11 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.kpref2 = pk.add(kpref2); o.sig2 = pk.add(sig2);
     const size_t t_q64 = pk.add(std::vector<double>(desc->charges, desc->charges + na));
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
-    const bool lists = sizeof(F) == 4;
-    size_t t_frac = 0, t_cells = 0, t_r2 = 0, t_nimg = 0, t_count = 0, t_order = 0, t_reach = 0, t_fr32 = 0;
-    if (lists) {
-        std::vector<double> frac(3 * na);
-        for (int fw = 0; fw < nfw; ++fw)
-            for (int32_t j = B->atom_offsets[fw]; j < B->atom_offsets[fw + 1]; ++j)
-                for (int r = 0; r < 3; ++r) {
-                    const double* iA = desc->invcells + 9 * fw;
-                    frac[3 * j + r] = iA[r] * desc->positions[3 * j] + iA[r + 3] * desc->positions[3 * j + 1] +
-                                      iA[r + 6] * desc->positions[3 * j + 2];
-                }
-        std::vector<double> cells64(desc->cells, desc->cells + 9 * nfw);
-        // each framework's atoms in type-major order (a stable counting sort): list entries of one
-        // type form one run; beside it the FP32 fractional coordinates in that order, which the
-        // list build's membership test reads coalesced
-        std::vector<int32_t> order(na), tstart(nt + 1);
-        std::vector<float4> fr32(na);
-        for (int fw = 0; fw < nfw; ++fw) {
-            const int32_t a0 = B->atom_offsets[fw], a1 = B->atom_offsets[fw + 1];
-            std::fill(tstart.begin(), tstart.end(), 0);
-            for (int32_t j = a0; j < a1; ++j) ++tstart[types[j] + 1];
-            for (int t = 0; t < nt; ++t) tstart[t + 1] += tstart[t];
-            for (int32_t j = a0; j < a1; ++j) order[a0 + tstart[types[j]]++] = j;
-            for (int32_t rk = a0; rk < a1; ++rk) {
-                const int32_t j = order[rk];
-                fr32[rk] = make_float4(float(frac[3 * j]), float(frac[3 * j + 1]), float(frac[3 * j + 2]), 0.f);
-            }
-        }
-        t_order = pk.add(order);
-        t_fr32 = pk.add(fr32);
-        t_frac = pk.add(frac); t_cells = pk.add(cells64); t_r2 = pk.add(radius2);
-        t_nimg = pk.add(nimg); t_reach = pk.add(reach); t_count = pk.reserve(sizeof(int32_t) * std::max(1, B->nbins));
-    }
+    if (lists) { t_order = pk.add(order); t_frac = pk.add(frac); }
     if (!pk.ok) return fail(ctx, PA_ERR_CUDA, "pinned staging allocation failed");
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.n, st));
     PA_CUDA(ctx, cudaMemcpyAsync(B->arena, ctx->h_stage, pk.n, cudaMemcpyHostToDevice, st));
+    PA_CUDA(ctx, cudaEventRecord(ctx->staged, st));
     char* base = static_cast<char*>(B->arena);
     B->kpref2 = reinterpret_cast<const double*>(base + o.kpref2);
     B->kpref2_h = kpref2;
@@ -520,30 +586,13 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     B->types0 = reinterpret_cast<const int32_t*>(base + o.types);
     if (lists) B->frac64 = reinterpret_cast<const double*>(base + t_frac);
     if (lists) {
-        // neighbour lists: count pass, padded offsets on the host, fill pass
-        pa::ListGeom g{};
+        // neighbour lists: the count pass (launched above), padded offsets on the host, fill pass
         g.frac = reinterpret_cast<const double*>(base + t_frac); g.charges = reinterpret_cast<const double*>(base + t_q64);
-        g.types = reinterpret_cast<const int32_t*>(base + o.types); g.cells = reinterpret_cast<const double*>(base + t_cells);
-        g.atom_offsets = reinterpret_cast<const int32_t*>(base + o.atom_offsets);
+        g.types = reinterpret_cast<const int32_t*>(base + o.types);
         g.order = reinterpret_cast<const int32_t*>(base + t_order);
-        g.fr32 = reinterpret_cast<const float4*>(base + t_fr32);
-        g.bin_dims = reinterpret_cast<const int32_t*>(base + o.bin_dims);
-        g.bin_base = reinterpret_cast<const int32_t*>(base + o.bin_base);
-        g.bin_fw = reinterpret_cast<const int32_t*>(base + o.bin_fw);
-        g.radius2 = reinterpret_cast<const double*>(base + t_r2); g.nimg = reinterpret_cast<const int32_t*>(base + t_nimg);
-        g.reach = reinterpret_cast<const float*>(base + t_reach);
-        g.counts = reinterpret_cast<int32_t*>(base + t_count);
-        if (B->nbins > 0) {
-            Timer tm(ctx, 4);
-            pa::k_lists<false><<<B->nbins, 256, 0, st>>>(g);
-            tm.stop(1);
-            PA_CUDA(ctx, cudaGetLastError());
-        }
-        std::vector<int32_t> counts(B->nbins);
-        if (B->nbins > 0)
-            PA_CUDA(ctx, cudaMemcpyAsync(counts.data(), g.counts, sizeof(int32_t) * B->nbins, cudaMemcpyDeviceToHost, st));
-        pa_status ws = wait_stream(ctx);
+        pa_status ws = wait_event(ctx, ctx->counted);
         if (ws != PA_OK) return ws;
+        const int32_t* counts = ctx->h_counts;
         std::vector<int32_t> loff(B->nbins + 1, 0);
         for (int32_t q2 = 0; q2 < B->nbins; ++q2) {
             int64_t padded = int64_t(std::ceil(counts[q2] / LIST_PAD) * LIST_PAD);
@@ -722,10 +771,14 @@ pa_status pa_context_create(int32_t device, pa_context** out) {
     if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PA_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->up, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->lists, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&ctx->lists, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->counted, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming) != cudaSuccess) {
         cudaStreamDestroy(ctx->own);
         if (ctx->aux) cudaStreamDestroy(ctx->aux);
         if (ctx->up) cudaEventDestroy(ctx->up);
+        if (ctx->lists) cudaEventDestroy(ctx->lists);
+        if (ctx->counted) cudaEventDestroy(ctx->counted);
         delete ctx;
         return PA_ERR_CUDA;
     }
@@ -743,6 +796,8 @@ pa_status pa_context_destroy(pa_context* ctx) {
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
     if (ctx->up) cudaEventDestroy(ctx->up);
     if (ctx->lists) cudaEventDestroy(ctx->lists);
+    if (ctx->counted) cudaEventDestroy(ctx->counted);
+    if (ctx->staged) cudaEventDestroy(ctx->staged);
     delete ctx;
     return PA_OK;
 }

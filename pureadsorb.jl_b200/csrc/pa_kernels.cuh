@@ -1073,6 +1073,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         const float z = dot3s(Af[2], Af[5], Af[8], e0, e1, e2);
         return dot3s(x, y, z, x, y, z) <= R2f;
     };
+    int32_t cnt_total = 0;  // count pass: this thread's entries
     // LIST_ATOMS consecutive atom ranks per thread, their loads issued together
     for (int32_t r0 = a0; r0 < a1; r0 += LIST_ATOMS * int32_t(blockDim.x)) {
         int32_t j[LIST_ATOMS], lo[LIST_ATOMS][3], hi[LIST_ATOMS][3];
@@ -1085,7 +1086,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
 #pragma unroll
             for (int r = 0; r < 3; ++r) { lo[u][r] = 0; hi[u][r] = -1; d[u][r] = 0.f; }
             if (rk < a1) {
-                j[u] = g.order[rk];
+                if constexpr (FILL) j[u] = g.order[rk];  // the count pass runs before `order` is uploaded
                 const float4 f = g.fr32[rk];
                 const float fv[3] = {f.x, f.y, f.z};
 #pragma unroll
@@ -1103,6 +1104,10 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
             for (int32_t n2 = lo[u][2]; n2 <= hi[u][2]; ++n2)
                 for (int32_t n1 = lo[u][1]; n1 <= hi[u][1]; ++n1)
                     for (int32_t n0 = lo[u][0]; n0 <= hi[u][0]; ++n0) cnt += inside(d[u], n0, n1, n2) ? 1 : 0;
+        if constexpr (!FILL) {  // the count pass only needs the bin's total: one reduction at the end
+            cnt_total += cnt;
+            continue;
+        }
         // ordered exclusive scan of the counts over the block
         int32_t incl = cnt;
 #pragma unroll
@@ -1151,7 +1156,17 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         if (threadIdx.x == 0) s_base += tot;
         __syncthreads();
     }
-    if (!FILL && threadIdx.x == 0) g.counts[bin] = s_base;
+    if constexpr (!FILL) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt_total += __shfl_xor_sync(0xffffffffu, cnt_total, o);
+        if (lane == 0) s_warp[wid] = cnt_total;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int32_t tot = 0;
+            for (int q = 0; q < 8; ++q) tot += s_warp[q];
+            g.counts[bin] = tot;
+        }
+    }
     if (FILL) {  // padding entries up to the next offset: far away, no charge
         const int32_t end = g.offsets[bin + 1];
         for (int32_t q = s_base + threadIdx.x; q < end; q += blockDim.x) {
