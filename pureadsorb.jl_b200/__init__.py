@@ -17,6 +17,7 @@ from .adjoint import WidomGrad, fold_replicas, widom_grad
 from .tune import TuneReport, autotune
 from . import fit
 from . import chain
+from . import cli
 from .chain import SystemState, insertion_constant_term, widom_along_chain, widom_chain
 from .widom import (B200Backend, WidomResult, _reduce, _widom, block_sums, boltzmann_weight, build_rejection_tables,
                     default_run, sys_of_index, system_counts, widom, widom_singlephase)
