@@ -701,32 +701,55 @@ __host__ __device__ inline SortView sort_view(const Work& w) {
     return SortView{w.bin_count, w.fine_start, w.bin_start, w.tile_start, w.counters, w.bin_of, w.slot, w.sorted};
 }
 
+// Each thread takes PA_SCAN_V consecutive elements per round (a serial prefix in registers), so
+// that a round of the block covers 1024 * PA_SCAN_V elements with one block-wide scan.
+#define PA_SCAN_V 8
 __device__ __forceinline__ void scan_body(SortView w, int32_t nbins, int32_t nsub, int32_t tile) {
     __shared__ int32_t s_warp[32];
     const int32_t nfine = nbins * nsub;
+    const int32_t per = int32_t(blockDim.x) * PA_SCAN_V;
     int32_t carry = 0;
-    for (int32_t base = 0; base < nfine; base += blockDim.x) {  // survivors per sub-bin -> starts
-        const int32_t f = base + threadIdx.x;
-        const int32_t c = f < nfine ? w.count[f] : 0;
+    for (int32_t base = 0; base < nfine; base += per) {  // survivors per sub-bin -> starts
+        const int32_t f0 = base + int32_t(threadIdx.x) * PA_SCAN_V;
+        int32_t v[PA_SCAN_V], sum = 0;
+#pragma unroll
+        for (int u = 0; u < PA_SCAN_V; ++u) {
+            v[u] = f0 + u < nfine ? w.count[f0 + u] : 0;
+            sum += v[u];
+        }
         int32_t tot;
-        const int32_t e = block_excl_scan(c, s_warp, &tot);
-        if (f < nfine) w.fine_start[f] = carry + e;
+        int32_t e = carry + block_excl_scan(sum, s_warp, &tot);
+#pragma unroll
+        for (int u = 0; u < PA_SCAN_V; ++u) {
+            if (f0 + u < nfine) w.fine_start[f0 + u] = e;
+            e += v[u];
+        }
         carry += tot;
     }
     if (threadIdx.x == 0) w.fine_start[nfine] = carry;
     __syncthreads();
     int32_t carry_t = 0;
-    for (int32_t base = 0; base < nbins; base += blockDim.x) {  // tiles per bin
-        const int32_t bn = base + threadIdx.x;
-        int32_t nt = 0;
-        if (bn < nbins) {
-            const int32_t s0 = w.fine_start[bn * nsub], s1 = w.fine_start[(bn + 1) * nsub];
-            w.bin_start[bn] = s0;
-            nt = (s1 - s0 + tile - 1) / tile;
+    for (int32_t base = 0; base < nbins; base += per) {  // tiles per bin
+        const int32_t b0 = base + int32_t(threadIdx.x) * PA_SCAN_V;
+        int32_t v[PA_SCAN_V], sum = 0;
+#pragma unroll
+        for (int u = 0; u < PA_SCAN_V; ++u) {
+            const int32_t bn = b0 + u;
+            v[u] = 0;
+            if (bn < nbins) {
+                const int32_t s0 = w.fine_start[bn * nsub], s1 = w.fine_start[(bn + 1) * nsub];
+                w.bin_start[bn] = s0;
+                v[u] = (s1 - s0 + tile - 1) / tile;
+            }
+            sum += v[u];
         }
         int32_t tt;
-        const int32_t et = block_excl_scan(nt, s_warp, &tt);
-        if (bn < nbins) w.tile_start[bn] = carry_t + et;
+        int32_t e = carry_t + block_excl_scan(sum, s_warp, &tt);
+#pragma unroll
+        for (int u = 0; u < PA_SCAN_V; ++u) {
+            if (b0 + u < nbins) w.tile_start[b0 + u] = e;
+            e += v[u];
+        }
         carry_t += tt;
     }
     if (threadIdx.x == 0) {
