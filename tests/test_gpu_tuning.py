@@ -40,6 +40,29 @@ def test_graph_replay_equals_direct_launch(pa, co2_batch):
     batch.drop_device()
 
 
+def test_call_right_after_upload_equals_resident(pa, co2_batch):
+    # the upload returns while the neighbour-list fill still runs on the context's second stream;
+    # a call issued at once (direct launch, then graph capture and replays of the same shape)
+    # must wait for the fill before its energy kernel, and so equal a call on a batch whose
+    # upload had finished
+    import torch
+
+    batch, guest = co2_batch
+    be = pa.B200Backend(0)
+    batch.drop_device()
+    batch.device(be.ctx)
+    torch.cuda.synchronize()
+    resident = _call(pa, batch, guest, be, 9)
+    be.ctx.set_tuning(use_graphs=True)
+    for _ in range(4):
+        batch.drop_device()
+        raw, ins = _call(pa, batch, guest, be, 9)  # uploads inside, then launches at once
+        for a, b in zip(raw, resident[0]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(ins["dU"], resident[1]["dU"])
+    batch.drop_device()
+
+
 @pytest.mark.parametrize("width,ctas", [(2.5, 4), (5.0, 6)])
 def test_bin_width_and_grid_keep_results(pa, co2_batch, width, ctas):
     batch, guest = co2_batch
