@@ -447,7 +447,7 @@ def main():
         sW, sUW = pa.block_sums(lse, sw, suw)
         res32 = pa._reduce(sW, sUW, cnt, kT32, float(np.float32(batch.volumes[0])), 1)
 
-        # roofline of the energy kernel: executed FP32 work per launch (model in DESIGN.md)
+        # roofline of the energy kernel: executed FP32 work per launch (the model below)
         ins = {}
         sample_n = 20_000
         pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=sample_n, seed=prm["seed"], nblocks=nblocks,
@@ -461,7 +461,7 @@ def main():
         nk = int(batch.k_offsets[1])
         kc = batch.kcoeffs
         rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
-        # executed FP32 work of k_energy32 per survivor (FMA = 2 flops; model stated in DESIGN.md):
+        # executed FP32 work of k_energy32 per survivor (FMA = 2 flops):
         # each of its N (insertion, site) items walks its bin's list, 8 flops per entry for the
         # distance, and 52 per in-cutoff pair (LJ 10 + screened Coulomb 38 + compensated add 4).
         # The reciprocal term (k_recip32: 10 per (k, site) + 7 per k for the recurrence, 25 per
