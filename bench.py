@@ -241,7 +241,8 @@ def chain_workload(pa, orc, backend, torch, stream, flush, no_cpu=False):
 
 def batched_workload(pa, backend, torch, stream, flush):
     """64 uneven frameworks, 2^20 insertions each, in one call (one persistent energy launch over
-    all frameworks' bins), batch tables built with device structure factors, autotuned, replayed
+    all frameworks' bins), batch tables built with device structure factors and self terms,
+    autotuned, replayed
     from a CUDA graph; FP32 against the plain FP64 form on 2^14 insertions per framework."""
     ctx = backend.ctx
     fws, ff, guest, ewald, prm = pa.synthetic.batched(T=np.float32)
@@ -317,7 +318,8 @@ def fitting_workload(pa, backend):
                                  sk=ctx.structure_factor, self_term=ctx.self_term)
     target_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor, self_term=ctx.self_term)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor, self_term=ctx.self_term,
+                          bounds=ctx.batch_bounds)
     build_s = time.perf_counter() - t0
     res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
                                lr=prm["lr"], seed=seed, backend=backend)

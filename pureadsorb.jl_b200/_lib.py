@@ -206,6 +206,12 @@ class Context:
         self.check(lib().pa_context_kernel_times(self.handle, ptr(ms), ptr(n)), "pa_context_kernel_times")
         return ms, n
 
+    def batch_bounds(self, batch):
+        """Hard-core bounds B_s of every framework of `batch` from the device
+        (pa_batch_hardcore_bounds), through the batch's upload to this context, which later calls
+        reuse; for FrameworkBatch(..., bounds=ctx.batch_bounds)."""
+        return batch.device(self).hardcore_bounds(batch.nframeworks())
+
     def self_term(self, ks, kpref, sites, charges):
         """Σ_k kpref |Σ_s q_s e^{i k·g_s(o)}|^2 for every orientation o of `sites` (norient x N x 3),
         on the device (pa_self_term)."""

@@ -72,10 +72,14 @@ class FrameworkBatch:
     the default evaluates them on the host in FP64 like the reference, and
     `sk=Context.structure_factor` runs the library's FP64 device kernel instead. `self_term`,
     likewise, computes the guest self term's per-orientation sums (ks, kpref, sites, charges) ->
-    array (without KE); `self_term=Context.self_term` runs them on the device.
+    array (without KE); `self_term=Context.self_term` runs them on the device. `bounds`, likewise,
+    computes the hard-core bounds B_s from the finished batch (batch -> array of one per
+    framework); `bounds=Context.batch_bounds` evaluates them on the device (FP64, equal to the
+    host's to rounding) through the batch's upload to that context, which later calls reuse.
     """
 
-    def __init__(self, fws, ff, guest, ewald, cellwidth=2, fullk=False, T=None, sk=None, self_term=None):
+    def __init__(self, fws, ff, guest, ewald, cellwidth=2, fullk=False, T=None, sk=None, self_term=None,
+                 bounds=None):
         fws = list(fws)
         if not fws:
             raise ArgumentError("FrameworkBatch needs at least one framework")
@@ -250,10 +254,11 @@ class FrameworkBatch:
         self._ff_names = list(ff.names)
         self._gcounts = gcounts
         self._offset_parts = offset_parts
-        self.bs = self._hardcore_bounds()
         self._device = {}
         self._desc = None      # desc() result; a FrameworkBatch is not modified after construction
         self._rejection = {}   # rejection tables per (kT, eps)
+        self.bs = (np.asarray(bounds(self), dtype=np.float64).reshape(-1) if bounds is not None
+                   else self._hardcore_bounds())
 
     def _hardcore_bounds(self):
         """B_s per framework (src/batch.jl:409-423)."""

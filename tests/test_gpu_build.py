@@ -25,3 +25,21 @@ def test_device_self_term_on_the_batched_frameworks(pa, backend):
     dev = pa.FrameworkBatch(fws, ff, guest, ewald, sk=backend.ctx.structure_factor, self_term=backend.ctx.self_term)
     assert np.allclose(dev.constant_offset, host.constant_offset, rtol=0, atol=1e-11)
     assert np.allclose(dev.self_term_halfrange, host.self_term_halfrange, rtol=1e-9, atol=1e-15)
+
+
+def test_device_hardcore_bounds_hook(pa, backend):
+    # FrameworkBatch(..., bounds=ctx.batch_bounds): B_s from the device through the batch's upload,
+    # equal to the host loop's to rounding; the upload is kept, and the rejection tables and a
+    # widom call on it work as with host bounds
+    fws, ff, guest, ewald, _ = pa.synthetic.batched(nfw=5, max_unit_atoms=300)
+    ctx = backend.ctx
+    host = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32)
+    dev = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, bounds=ctx.batch_bounds)
+    assert len(dev._device) == 1
+    fin = np.isfinite(host.bs)
+    assert np.array_equal(fin, np.isfinite(dev.bs))
+    np.testing.assert_allclose(dev.bs[fin], host.bs[fin], rtol=1e-10, atol=1e-12)
+    raw = pa._widom(dev, guest, reject=True, T=298.15, ninsert=20_000, seed=3, nblocks=4, backend=backend,
+                    segment_range=(0, 0))
+    assert np.all(np.asarray(raw[3]) > 0)
+    dev.drop_device()

@@ -143,3 +143,18 @@ def test_default_run_and_counts(pa):
     assert pa.default_run(1_000_000, 1) == 256
     assert pa.default_run(100, 7) == 3
     assert pa.default_run(3, 7) == 1
+
+
+def test_bounds_hook_sets_the_batch_bounds(pa):
+    # the `bounds` hook receives the finished batch and its result becomes B_s
+    fws, ff, guest, ewald, _ = pa.synthetic.co2()
+    host = pa.FrameworkBatch(fws, ff, guest, ewald)
+    seen = []
+
+    def hook(b):
+        seen.append(b)
+        return np.full(b.nframeworks(), 1.25)
+
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, bounds=hook)
+    assert len(seen) == 1 and seen[0] is b
+    assert np.array_equal(b.bs, [1.25]) and np.array_equal(b.positions, host.positions)
