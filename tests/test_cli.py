@@ -110,3 +110,15 @@ def test_module_entry(files):
     assert p.returncode == 0, p.stderr
     rec = json.loads(p.stdout.strip().splitlines()[0])
     assert rec["nsamples"] == 20000 and rec["K_H"] > 0
+
+
+def test_two_frameworks_each_replicated(pa, files, tmp_path):
+    # a second, larger CIF: each framework gets its own smallest replication that passes the guard
+    big = CIF.replace("_cell_length_a 13.0", "_cell_length_a 29.0")
+    p = tmp_path / "big.cif"
+    p.write_text(big)
+    a = pa.cli.parser().parse_args(args_for(files) + ["--cif", str(p)])
+    fws, ff, guest, ewald = pa.cli.build_inputs(a)
+    assert [fw.replication for fw in fws] == [(2, 2, 2), (1, 2, 2)]
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald)
+    assert batch.nsys == 2 and batch.nframeworks() == 2
