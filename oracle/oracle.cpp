@@ -72,29 +72,19 @@ const double SIN64[9] = {1.5707963267948966, -0.6459640975062463, 0.079692626246
 const double COS64[10] = {1.0, -1.2337005501361697, 0.25366950790104803, -0.02086348076335296,
                           0.0009192602748394266, -2.5202042373060607e-05, 4.710874778818172e-07,
                           -6.386603083791852e-09, 6.565963114979473e-11, -5.294400200734623e-13};
-const float SIN32[6] = {1.5707963705062866f, -0.6459640860557556f, 0.07969262450933456f,
-                        -0.004681753925979137f, 0.00016044118092395365f, -3.598843250074424e-06f};
-const float COS32[7] = {1.0f, -1.2337005138397217f, 0.25366950035095215f, -0.020863480865955353f,
-                        0.0009192602592520416f, -2.520204179745633e-05f, 4.710874748070637e-07f};
-
 template <typename F> struct Poly;
 template <> struct Poly<double> {
     static double s(double z) { double p = SIN64[8]; for (int k = 7; k >= 0; --k) p = std::fma(p, z, SIN64[k]); return p; }
     static double c(double z) { double p = COS64[9]; for (int k = 8; k >= 0; --k) p = std::fma(p, z, COS64[k]); return p; }
 };
-template <> struct Poly<float> {
-    static float s(float z) { float p = SIN32[5]; for (int k = 4; k >= 0; --k) p = std::fmaf(p, z, SIN32[k]); return p; }
-    static float c(float z) { float p = COS32[6]; for (int k = 5; k >= 0; --k) p = std::fmaf(p, z, COS32[k]); return p; }
-};
 
-template <typename F>
-inline void sincos2pi(F u, F* sn, F* cs) {
-    F y = u * F(4);
-    F q = std::nearbyint(y);  // round half to even (default rounding mode)
-    F r = y - q;
-    F z = r * r;
-    F s = r * Poly<F>::s(z);
-    F c = Poly<F>::c(z);
+inline void sincos2pi(double u, double* sn, double* cs) {
+    double y = u * 4.0;
+    double q = std::nearbyint(y);  // round half to even (default rounding mode)
+    double r = y - q;
+    double z = r * r;
+    double s = r * Poly<double>::s(z);
+    double c = Poly<double>::c(z);
     int qi = int(q) & 3;
     switch (qi) {
         case 0: *sn = s; *cs = c; break;
@@ -102,6 +92,14 @@ inline void sincos2pi(F u, F* sn, F* cs) {
         case 2: *sn = -s; *cs = -c; break;
         default: *sn = -c; *cs = s; break;
     }
+}
+// FP32 (Float32 sinpi(2u), cospi(2u), src/rng.jl:126-129): the FP64 values rounded once, which is
+// the correctly rounded result for every FP32 uniform; zeros as +0
+inline void sincos2pi(float u, float* sn, float* cs) {
+    double s, c;
+    sincos2pi(double(u), &s, &c);
+    *sn = float(s) + 0.0f;
+    *cs = float(c) + 0.0f;
 }
 
 template <typename F> inline F unit(uint64_t raw);

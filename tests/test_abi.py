@@ -34,6 +34,18 @@ def test_host_pose_stream_matches_oracle(pa, orc):
             assert np.array_equal(rr, r[k - 1]) and np.array_equal(qq, q[k - 1])
 
 
+def test_host_pose_stream_matches_golden_quaternions(pa):
+    # the library's FP32 quaternions equal the independent Python/mpmath restatement bit for bit
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rng_kat.json")) as fh:
+        kat = json.load(fh)
+    for c in kat["pose_stream"]:
+        _, qq = pa._lib.pose_host(32, int(c["seed"]), c["s"], c["k"])
+        assert qq.astype(np.float32).view(np.uint32).tolist() == c["quat_f32_bits"]
+
+
 def test_segment_count_and_combine_host(pa):
     L = pa._lib.lib()
     n = pa._lib.ctypes.c_int64()

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 from scipy.special import erfc
 
-from conftest import kT_of, oracle_view, reference_data
+from conftest import kT_of, oracle_view, reference_data, rubtak_case
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -29,6 +29,9 @@ def test_rng_golden_vectors(orc):
             assert L.or_unit_f64(raw) == float.fromhex(c["u64"][d])
             bits = np.array([L.or_unit_f32(raw)], dtype=np.float32).view(np.uint32)[0]
             assert int(bits) == c["u32_bits"][d]
+        # the FP32 quaternion, bit for bit (correctly rounded sinpi/cospi)
+        _, q = orc.poses(32, seed, s, k, 1)
+        assert q[0].astype(np.float32).view(np.uint32).tolist() == c["quat_f32_bits"]
     for m in kat["mulhi64"]:
         assert L.or_mulhi64(int(m["a"]), int(m["b"])) == int(m["hi"])
 
@@ -77,23 +80,70 @@ def test_quaternions_uniform_on_so3(orc, prec):
     assert np.all(np.abs(q.mean(axis=0)) < 5 * math.sqrt(0.25 / n))
 
 
-@pytest.mark.parametrize("prec", [64, 32])
-def test_sincos2pi_accuracy(orc, prec):
+def test_sincos2pi_accuracy_f64(orc):
     n = 100_001
-    if prec == 64:
-        u = np.linspace(0, 1, n, endpoint=False)
-        s, c = np.zeros(n), np.zeros(n)
-        orc.lib().or_sincos2pi_f64(orc.P(u), n, orc.P(s), orc.P(c))
-        tol = 1.2e-15  # the numpy reference itself rounds 2*pi*u (up to ~6e-16 near u = 1)
-    else:
-        u = np.linspace(0, 1, n, endpoint=False).astype(np.float32)
-        s, c = np.zeros(n, np.float32), np.zeros(n, np.float32)
-        orc.lib().or_sincos2pi_f32(orc.P(u), n, orc.P(s), orc.P(c))
-        tol = 2.5e-7
-    ref_s = np.sin(2 * np.pi * u.astype(np.float64))
-    ref_c = np.cos(2 * np.pi * u.astype(np.float64))
-    assert np.max(np.abs(s - ref_s)) < tol
-    assert np.max(np.abs(c - ref_c)) < tol
+    u = np.linspace(0, 1, n, endpoint=False)
+    s, c = np.zeros(n), np.zeros(n)
+    orc.lib().or_sincos2pi_f64(orc.P(u), n, orc.P(s), orc.P(c))
+    tol = 1.2e-15  # the numpy reference itself rounds 2*pi*u (up to ~6e-16 near u = 1)
+    assert np.max(np.abs(s - np.sin(2 * np.pi * u))) < tol
+    assert np.max(np.abs(c - np.cos(2 * np.pi * u))) < tol
+
+
+def test_sincos2pi_f32_correctly_rounded_exhaustive(orc):
+    # Float32 sinpi(2u) / cospi(2u) of every FP32 uniform u = k 2^-24 (src/rng.jl:126-129): the
+    # oracle's (and the library's) FP32 values must be the correctly rounded ones, +0 for zeros.
+    # Reference: sin/cos((pi/2) r) in x87 extended precision (64-bit significand) after the exact
+    # quadrant reduction 4u = q + r, rounded to FP32; any input whose extended value lies within
+    # 1e-17 (relative) of an FP32 rounding midpoint is settled with mpmath at 50 digits.
+    import mpmath as mp
+
+    k = np.arange(2**24, dtype=np.int64)
+    u = (k.astype(np.float64) * 2.0**-24).astype(np.float32)
+    s, c = np.zeros(2**24, np.float32), np.zeros(2**24, np.float32)
+    orc.lib().or_sincos2pi_f32(orc.P(u), 2**24, orc.P(s), orc.P(c))
+    L = np.longdouble
+    y = 4 * k  # 4u in units of 2^-24
+    q = (y + 2**23) >> 24  # rint(4u), ties (r = 1/2) to even below
+    q = np.where(((y & (2**24 - 1)) == 2**23) & ((q & 1) == 1), q - 1, q)
+    r = (y - (q << 24)).astype(L) * L(2.0**-24)
+    hp = L("1.570796326794896619231321691639751442")
+    sr, cr = np.sin(hp * r), np.cos(hp * r)
+    qi = q & 3
+    ref = {"sin": np.select([qi == 0, qi == 1, qi == 2], [sr, cr, -sr], -cr),
+           "cos": np.select([qi == 0, qi == 1, qi == 2], [cr, -sr, -cr], sr)}
+    mp.mp.dps = 50
+    for name, got in (("sin", s), ("cos", c)):
+        e = ref[name]
+        r32 = e.astype(np.float32) + np.float32(0)
+        lo = np.nextafter(r32, np.float32(-np.inf)).astype(L)
+        hi = np.nextafter(r32, np.float32(np.inf)).astype(L)
+        m = r32.astype(L)
+        dist = np.minimum(np.abs(e - (m + lo) / 2), np.abs(e - (m + hi) / 2)) / np.maximum(np.abs(e), L(1e-30))
+        near = np.nonzero(dist < 1e-17)[0]
+        for i in near:
+            f = mp.sinpi if name == "sin" else mp.cospi
+            r32[i] = round_f32(f(2 * mp.mpf(float(u[i]))))
+        assert np.array_equal(got.view(np.uint32), r32.view(np.uint32)), name
+    # spot checks of the extended-precision reference itself against mpmath
+    for i in np.random.default_rng(3).integers(0, 2**24, 64):
+        assert s[i].view(np.uint32) == round_f32(mp.sinpi(2 * mp.mpf(float(u[i])))).view(np.uint32)
+        assert c[i].view(np.uint32) == round_f32(mp.cospi(2 * mp.mpf(float(u[i])))).view(np.uint32)
+
+
+def round_f32(v):
+    """The FP32 value nearest to the mpmath number v (ties to even), zero as +0."""
+    f = np.float32(float(v))
+    cands = [np.nextafter(f, np.float32(-np.inf)), f, np.nextafter(f, np.float32(np.inf))]
+    d = [abs(v - mp_of(x)) for x in cands]
+    best = min(range(3), key=lambda i: (d[i], int(cands[i].view(np.uint32)) & 1))
+    return cands[best] + np.float32(0)
+
+
+def mp_of(x):
+    import mpmath as mp
+
+    return mp.mpf(float(x))
 
 
 # ---------------------------------------------------------- Ewald (test/ewald_tests.jl)
@@ -494,12 +544,26 @@ def test_single_lj_atom_radial_integral(pa, orc):
 
 
 # ---------------------------------------------------------- RUBTAK (reference data files)
-def test_rubtak_batch_known_answers(pa, orc):
-    # test/structure_tests.jl:1-11, test/batch_tests.jl:1-30, 71-88:
-    # 114 atoms, q1 = 2.38565, 3,078 atoms after 3x3x3, 190 coupled k-vectors, dropped |S| < 1e-9
+def test_rubtak_readers_reproduce_fixture(pa):
+    # the readers on the reference's own files give the committed fixture's values exactly
     fw = pa.read_cif(reference_data("RUBTAK.cif"))
     ff = pa.read_forcefield(reference_data("trappe.yaml"))
     g = pa.read_guest(reference_data("co2.yaml"), ff)
+    (sc,), ffx, gx, _, d = rubtak_case(pa)
+    assert np.array_equal(fw.frac, np.array(d["framework"]["frac"])) and fw.symbols == d["framework"]["symbols"]
+    assert np.array_equal(fw.charges, np.array(d["framework"]["charges"]))
+    for n in ffx.names:
+        i, j = ff.typeindex(n) - 1, ffx.typeindex(n) - 1
+        assert ff.sigma[i, i] == ffx.sigma[j, j] and ff.epsilon[i, i] == ffx.epsilon[j, j]
+    assert np.array_equal(g.sites, gx.sites) and np.array_equal(g.charges, gx.charges)
+
+
+def test_rubtak_batch_known_answers(pa, orc):
+    # test/structure_tests.jl:1-11, test/batch_tests.jl:1-30, 71-88:
+    # 114 atoms, q1 = 2.38565, 3,078 atoms after 3x3x3, 190 coupled k-vectors, dropped |S| < 1e-9
+    (sc,), ff, g, _, d = rubtak_case(pa)
+    f = d["framework"]
+    fw = pa.Framework(np.array(f["cell"]), np.array(f["frac"]), f["labels"], f["symbols"], np.array(f["charges"]))
     assert pa.natoms(fw) == 114 and fw.symbols[0] == "Zr" and fw.charges[0] == pytest.approx(2.38565)
     assert abs(pa.total_charge(fw)) < 1e-3
     sc = pa.replicate(fw, (3, 3, 3))
