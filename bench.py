@@ -55,7 +55,8 @@ def parse():
 
 class Clocks:
     """SM clock and throttle reasons sampled through NVML (read-only) every 5 ms during the timed
-    region; falls back to nvidia-smi when NVML is unavailable."""
+    region; the summary reports "unsampled" when NVML is unavailable. The NVML device is found by
+    the CUDA device's PCI address, since NVML's indices ignore CUDA_VISIBLE_DEVICES."""
 
     REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
@@ -63,13 +64,20 @@ class Clocks:
         self.device = device
         self.samples = []  # (sm MHz, reason bits)
         self.max_mhz = None
+        self.pci = None
         self.stop = threading.Event()
+
+    def handle(self, pynvml):
+        import torch
+        p = torch.cuda.get_device_properties(self.device)
+        self.pci = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return pynvml.nvmlDeviceGetHandleByPciBusId(self.pci.encode())
 
     def __enter__(self):
         try:
             import pynvml
             pynvml.nvmlInit()
-            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            h = self.handle(pynvml)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
 
             def poll():
@@ -97,7 +105,7 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
         reasons = sorted({name for _, bits in self.samples for bit, name in self.REASONS.items() if bits & bit})
         return {"sm_mhz": float(np.median([m for m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "pci_bus_id": self.pci}
 
 
 def load_peaks():
@@ -145,21 +153,66 @@ def count_pairs(batch, poses):
     return nl / n, ne / n
 
 
-def cpu_baseline_port(pa, orc, batch, guest, ninsert_full, target_s=12.0, nthreads=0):
+class OracleWorkload:
+    """The CO2 workload as the CPU implementation sees it: the oracle's own FrameworkBatch builder
+    (dedup, compact types, cell sort, k tables, self term, constant offset, B_s and kmin) and its
+    own rejection tables, from the same synthetic frameworks, force field and guest. Nothing of
+    the product library is loaded on this path; `product_library_loaded` checks that."""
+
+    def __init__(self, pa, orc, T_K=298.15):
+        fws, ff, guest, ewald, prm = pa.synthetic.co2(T=np.float64)
+        frames = [(fw.cell, fw.frac, [ff.typeindex(s + "_") for s in fw.symbols], fw.charges, fw.replication)
+                  for fw in fws]
+        # the self term's orientations: the pose stream's quaternions for its fixed seed
+        quats = orc.poses(64, pa.batch.SELF_TERM_SEED, 0, 1, pa.batch.SELF_TERM_NORIENT)[1]
+        self.orc, self.prm = orc, prm
+        self.b = orc.OracleBatch(frames, (np.diag(ff.sigma), np.diag(ff.epsilon), ff.cutoff, ff.tail),
+                                 (guest.sites, guest.types, guest.charges), ewald.cutoff, ewald.precision, 2.0,
+                                 False, quats)
+        self.v, self.keep = orc.view(self.b, guest.sites, guest.charges, ff.cutoff, ewald.cutoff)
+        self.kT = float(np.float64(pa.KB * T_K))
+        self.natoms = int(len(self.b.positions))
+        self.coupled_k = int(self.b.k_offsets[-1])
+
+    def rejection_tables(self):
+        """The rejection radii of one call, recomputed like every reference widom call does."""
+        return self.orc.rejection_tables(self.v, self.b.bs, self.b.kmin, self.kT, float(np.finfo(np.float64).eps))
+
+    def widom(self, n, nthreads=0):
+        rho2, reach0 = self.rejection_tables()
+        run = max(1, min(256, n // 4))  # default_run for one system (src/widom.jl:39)
+        return self.orc.widom(self.v, 64, self.kT, n, self.prm["seed"], self.prm["nblocks"], run, True, rho2, reach0,
+                              nthreads=nthreads, want_insertions=False)
+
+
+def product_library_loaded():
+    """True when this process has mapped the product's CUDA library."""
+    try:
+        with open("/proc/self/maps") as fh:
+            return "libpureadsorb_b200.so" in fh.read()
+    except OSError:
+        return False
+
+
+def cpu_baseline_port(wl, ninsert_full, target_s=12.0, nthreads=0):
     """Times the oracle (FP64 C++ restatement of the reference CPU path, OpenMP over the host
-    cores) on a bounded sample of the same workload; returns (insertions/s, sample size, cores)."""
-    v, keep = orc.view(batch, batch.guest_sites_orig, batch.guest_charges_orig, batch.cutoff, batch.ewald_cutoff)
-    kT = float(np.float64(pa.KB * 298.15))
-    rho2, reach0 = pa.build_rejection_tables(batch, kT)
+    cores) on a bounded sample of the same workload, rejection tables included in every call;
+    returns (insertions/s, sample size, cores)."""
     n = 4000
     while True:
-        run = pa.default_run(n, 1)
         t0 = time.perf_counter()
-        orc.widom(v, 64, kT, n, 42, 10, run, True, rho2, reach0, nthreads=nthreads, want_insertions=False)
+        wl.widom(n, nthreads=nthreads)
         dt = time.perf_counter() - t0
         if dt > 0.25 * target_s or n >= ninsert_full:
             return n / dt, n, (nthreads or os.cpu_count())
         n = int(min(ninsert_full, n * max(2.0, 0.5 * target_s / max(dt, 1e-3))))
+
+
+def bench_config(ninsert, world, natoms, coupled_k, prm):
+    """The workload description both arms print (same keys and values for the same run)."""
+    return {"workload": WORKLOAD, "ninsert_per_gpu": ninsert, "ninsert_total": ninsert * world, "natoms": natoms,
+            "guest_sites": 3, "coupled_k": coupled_k, "nblocks": prm["nblocks"], "seed": prm["seed"],
+            "T_K": prm["T"], "l2": "flushed between steps (256 MB write)", "parallelism": f"shard{world}"}
 
 
 def chain_workload(pa, orc, backend, torch, stream, flush, no_cpu=False):
@@ -344,20 +397,26 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        batch, guest, prm = workload(pa, np.float64)
+        # the reference is Julia (no toolchain here): its CPU path is the oracle, the C++ FP64
+        # restatement, with the oracle's own batch builder and rejection tables
+        wl = OracleWorkload(pa, orc)
         rates = []
         for i in range(args.warmup + args.steps):
-            r, n, cores = cpu_baseline_port(pa, orc, batch, guest, args.ninsert, target_s=8.0)
+            r, n, cores = cpu_baseline_port(wl, args.ninsert, target_s=8.0)
             if i >= args.warmup:
                 rates.append(r)
+        if product_library_loaded():
+            raise RuntimeError("the reference arm loaded the product library")
         v = float(np.median(rates))
         line = {"metric": METRIC, "value": v, "unit": "insertions/s",
                 "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "ninsert": args.ninsert, "sample_insertions": n},
+                "higher_is_better": True, "scaling": "weak", "dtype": "f64", "data": "synthetic",
+                "config": bench_config(args.ninsert, max(1, args.gpus), wl.natoms, wl.coupled_k, wl.prm),
                 "cpu_baseline": {"value": v, "unit": "insertions/s", "cores": cores, "kind": "port",
-                                 "sample": f"{n} insertions of the workload per step (two-phase, FP64)"},
+                                 "sample": f"{n} insertions of the workload per step (two-phase, FP64, rejection "
+                                           "tables rebuilt per call, oracle batch builder; OpenMP)"},
                 "e2e": {"value": v, "unit": "insertions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "product_library_loaded": False,
                 "vs_baseline": None}
         print(json.dumps(line))
         return 0
@@ -488,7 +547,7 @@ def main():
         fp64 = None
         if not args.no_fp64:
             b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
-            n64 = min(ninsert, 200_000)
+            n64 = args.ninsert
             for _ in range(2):
                 pa.widom(b64, guest, T=prm["T"], ninsert=n64, seed=prm["seed"], nblocks=nblocks, backend=backend)
             torch.cuda.synchronize()
@@ -509,7 +568,9 @@ def main():
         h2d = sum(a.nbytes for a in batch.desc()[1].values()) + 8 * (len(batch.guest_types) * len(batch.sigma) + 3)
         d2h = 3 * 8 * nseg + 4 * 8 * nblocks
         for i in range(args.warmup + max(3, args.steps // 2)):
+            # every step re-uploads the batch and rebuilds its descriptor and rejection tables
             batch.drop_device()
+            batch.drop_host_caches()
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -556,19 +617,16 @@ def main():
 
         cpu = None
         if not args.no_cpu:
-            b64 = pa.FrameworkBatch(*pa.synthetic.co2(T=np.float64)[:4])
-            r, n, cores = cpu_baseline_port(pa, orc, b64, guest, args.ninsert)
+            r, n, cores = cpu_baseline_port(OracleWorkload(pa, orc), args.ninsert)
             cpu = {"value": r, "unit": "insertions/s", "cores": cores, "kind": "port",
-                   "sample": f"{n} insertions of the workload (FP64 oracle, two-phase, OpenMP)"}
+                   "sample": f"{n} insertions of the workload (FP64 oracle, two-phase, rejection tables rebuilt "
+                             "per call, OpenMP)"}
 
         line = {"metric": METRIC,
                 "value": value, "unit": "insertions/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "ninsert_per_gpu": args.ninsert,
-                           "ninsert_total": ninsert, "natoms": int(len(batch.positions)), "guest_sites": 3,
-                           "coupled_k": nk, "nblocks": nblocks, "seed": prm["seed"], "T_K": prm["T"],
-                           "l2": "flushed between steps (256 MB write)", "parallelism": f"shard{world}"},
+                "config": bench_config(args.ninsert, world, int(len(batch.positions)), nk, prm),
                 "result": {"mu_ex": res32.mu_ex, "mu_ex_err": res32.mu_ex_err, "K_H": res32.K_H,
                            "K_H_err": res32.K_H_err, "q_st": res32.q_st, "q_st_err": res32.q_st_err},
                 "clocks": clk.summary(),

@@ -386,6 +386,12 @@ class FrameworkBatch:
             dev.free()
         self._device.clear()
 
+    def drop_host_caches(self):
+        """Forgets the cached C-ABI descriptor and the per-(kT, eps) rejection tables, so the next
+        call rebuilds both as a reference widom call does (src/widom.jl:382)."""
+        self._desc = None
+        self._rejection = {}
+
 
 def nframeworks(batch):
     return batch.nframeworks()
