@@ -78,6 +78,23 @@ typedef struct pa_tuning {
 pa_status pa_context_set_tuning(pa_context* ctx, const pa_tuning* tuning);
 pa_status pa_context_get_tuning(const pa_context* ctx, pa_tuning* tuning);
 
+/* Which parts of the FP32 path run in FP64 (no counterpart in the reference, whose Float32 batch
+ * computes everything in Float32). near_radius: pairs of an (insertion, site) item closer than
+ * this (Å), and pairs whose FP32 distance lies within 4e-6 rc^2 of a cutoff rc^2 (where FP32
+ * rounding could flip the cutoff test), are evaluated in FP64 from FP64 list coordinates, FP64
+ * site geometry and FP64 pair tables; every other pair stays FP32; 0 turns the FP64 pairs (and
+ * the cutoff bands) off. fp64_reciprocal: 1 evaluates the reciprocal cross term (phase factors,
+ * row recurrences, sums) in FP64, 0 in FP32. Applies to every later pa_widom / pa_widom_grad /
+ * pa_widom_static call of the context; the defaults are PA_DEFAULT_NEAR_RADIUS and 1. */
+#define PA_DEFAULT_NEAR_RADIUS 6.0
+typedef struct pa_fp32_split {
+    double near_radius;
+    int32_t fp64_reciprocal;
+    int32_t reserved;           /* 0 */
+} pa_fp32_split;
+pa_status pa_context_set_fp32_split(pa_context* ctx, const pa_fp32_split* split);
+pa_status pa_context_get_fp32_split(const pa_context* ctx, pa_fp32_split* split);
+
 /*
  * The fields of a `FrameworkBatch` (src/batch.jl:72-104), as raw arrays. natoms = Σ atoms
  * (atom_offsets[nfw]); nk = Σ k-vectors (k_offsets[nfw]); N = nguest; nt = ntypes.

@@ -60,6 +60,10 @@ class InsertionOut(ctypes.Structure):
     _fields_ = [("dU", _p), ("flags", _p), ("poses", _p)]
 
 
+class Fp32Split(ctypes.Structure):
+    _fields_ = [("near_radius", _f64), ("fp64_reciprocal", _i32), ("reserved", _i32)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("bin_width", _f64), ("ctas_per_sm", _i32), ("use_graphs", _i32)]
 
@@ -79,6 +83,8 @@ SIGNATURES = [
     ("pa_context_kernel_times", _i32, [_p, _p, _p]),
     ("pa_context_set_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
     ("pa_context_get_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
+    ("pa_context_set_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
+    ("pa_context_get_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
     ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
     ("pa_batch_free", _i32, [_p]),
     ("pa_batch_set_pair_tables", _i32, [_p, _p, _p, _p, _p]),
@@ -199,6 +205,22 @@ class Context:
         t = Tuning()
         self.check(lib().pa_context_get_tuning(self.handle, ctypes.byref(t)), "pa_context_get_tuning")
         return t
+
+    def set_fp32_split(self, near_radius=None, fp64_reciprocal=None):
+        """FP32 path (pa_fp32_split): pairs closer than near_radius (Å), and pairs at a cutoff's
+        rounding band, are evaluated in FP64 (0 keeps every pair in FP32); fp64_reciprocal selects
+        the FP64 reciprocal term. Arguments left None keep their values."""
+        sp = self.fp32_split()
+        if near_radius is not None:
+            sp.near_radius = float(near_radius)
+        if fp64_reciprocal is not None:
+            sp.fp64_reciprocal = int(bool(fp64_reciprocal))
+        self.check(lib().pa_context_set_fp32_split(self.handle, ctypes.byref(sp)), "pa_context_set_fp32_split")
+
+    def fp32_split(self):
+        sp = Fp32Split()
+        self.check(lib().pa_context_get_fp32_split(self.handle, ctypes.byref(sp)), "pa_context_get_fp32_split")
+        return sp
 
     def kernel_times(self):
         ms = np.zeros(8)

@@ -80,6 +80,7 @@ struct pa_context {
     std::vector<int32_t> up_chain_goff, up_chain_gtype;
     // launch choices, the replayable graph of the last call's device sequence and its key
     pa_tuning tuning{0.0, 0, 0};
+    pa_fp32_split split{PA_DEFAULT_NEAR_RADIUS, 1, 0};
     cudaGraphExec_t gexec = nullptr;
     std::vector<unsigned char> gkey, last_key;  // key of the captured graph, and of the last call
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
@@ -342,7 +343,8 @@ pa_status wait_stream(pa_context* ctx) {
 struct Slots {
     size_t framework_of, cells, invcells, alphas, const_offset, atom_offsets, atoms, types, ncells, cell_offsets,
         cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, kpref2, sig2, eps4, bin_dims, bin_base, bin_fw;
-    size_t list_offsets, list_xyzq, list_type, list_atom, list_runs;  // offsets inside the list allocation
+    size_t list_offsets, list_xyzq, list_type, list_atom, list_runs, list_xyzq64;  // inside the list allocation
+    size_t cells64, invcells64, sig2_64, eps4_64;
 };
 
 template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc, const Slots& o) {
@@ -385,6 +387,21 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     d.list_atom = l ? reinterpret_cast<const int32_t*>(l + o.list_atom) : nullptr;
     d.list_runs = l ? reinterpret_cast<const int2*>(l + o.list_runs) : nullptr;
     d.runs_per_bin = B->runs_per_bin;
+    d.list_xyzq64 = l ? reinterpret_cast<const double4*>(l + o.list_xyzq64) : nullptr;
+    d.cells64 = reinterpret_cast<const double*>(a + o.cells64);
+    d.invcells64 = reinterpret_cast<const double*>(a + o.invcells64);
+    d.sig2_64 = reinterpret_cast<const double*>(a + o.sig2_64);
+    d.eps4_64 = reinterpret_cast<const double*>(a + o.eps4_64);
+    for (int q = 0; q < B->nguest; ++q) {
+        for (int r = 0; r < 3; ++r) d.gsite64[3 * q + r] = desc->guest_sites[3 * q + r];
+        d.gq64[q] = desc->guest_charges[q];
+    }
+    d.rl2_64 = desc->cutoff * desc->cutoff;
+    d.re2_64 = desc->ewald_cutoff * desc->ewald_cutoff;
+    d.rn2 = F(0);  // set per call from the context's split
+    d.recip64 = 0;
+    d.rl2_lo = d.rl2_hi = d.rl2;
+    d.re2_lo = d.re2_hi = d.re2;
 }
 
 template <typename F>
@@ -547,6 +564,7 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         }
     }
     std::vector<F> sig2(N * nt), eps4(N * nt);
+    std::vector<double> sig2_64(N * nt), eps4_64(N * nt);
     B->site_sigma.assign(N * nt, 0.0);
     B->site_eps.assign(N * nt, 0.0);
     for (int a = 0; a < N; ++a) {
@@ -555,6 +573,8 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             double s = desc->sigma[gt + nt * t], e = desc->epsilon[gt + nt * t];
             sig2[a * nt + t] = F(s * s);
             eps4[a * nt + t] = F(4 * e);
+            sig2_64[a * nt + t] = s * s;
+            eps4_64[a * nt + t] = 4 * e;
             B->site_sigma[a * nt + t] = s;
             B->site_eps[a * nt + t] = e;
         }
@@ -572,6 +592,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.kcoef = pk.add(kcoef4); o.kstep = pk.add(kstep); o.kS2 = pk.add(kS2); o.kpref2 = pk.add(kpref2); o.sig2 = pk.add(sig2);
     const size_t t_q64 = pk.add(std::vector<double>(desc->charges, desc->charges + na));
     o.eps4 = pk.add(eps4); o.bin_dims = pk.add(bdims); o.bin_base = pk.add(bbase); o.bin_fw = pk.add(bfw);
+    o.cells64 = pk.add(std::vector<double>(desc->cells, desc->cells + 9 * nfw));
+    o.invcells64 = pk.add(std::vector<double>(desc->invcells, desc->invcells + 9 * nfw));
+    o.sig2_64 = pk.add(sig2_64); o.eps4_64 = pk.add(eps4_64);
     if (lists) { t_order = pk.add(order); t_frac = pk.add(frac); }
     if (!pk.ok) return fail(ctx, PA_ERR_CUDA, "pinned staging allocation failed");
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.n, st));
@@ -618,11 +641,13 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
         }
         B->runs_per_bin = tmax + 2;
         o.list_runs = up256(o.list_atom + sizeof(int32_t) * nent);
-        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_runs + sizeof(int2) * size_t(std::max(1, B->nbins)) * B->runs_per_bin, st));
+        o.list_xyzq64 = up256(o.list_runs + sizeof(int2) * size_t(std::max(1, B->nbins)) * B->runs_per_bin);
+        PA_CUDA(ctx, cudaMallocAsync(&B->lists, o.list_xyzq64 + sizeof(double4) * nent, st));
         PA_CUDA(ctx, cudaMemcpyAsync(B->lists, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st));
         char* lb = static_cast<char*>(B->lists);
         g.offsets = reinterpret_cast<const int32_t*>(lb + o.list_offsets);
         g.xyzq = reinterpret_cast<float4*>(lb + o.list_xyzq);
+        g.xyzq64 = reinterpret_cast<double4*>(lb + o.list_xyzq64);
         g.type_out = reinterpret_cast<int32_t*>(lb + o.list_type);
         g.atom_out = reinterpret_cast<int32_t*>(lb + o.list_atom);
         if (B->nbins > 0) {
@@ -704,7 +729,8 @@ cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Wor
 template <int NS>
 cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallArgs& ca, const pa::Work& w,
                                  int32_t num_sms, cudaStream_t st) {
-    if (v32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+    if (v32.has_charge && v32.recip64) pa::k_recip64<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+    else if (v32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
     pa::k_combine<NS><<<unsigned((ca.n_act + 255) / 256), 256, 0, st>>>(v32, ca, w);
     return cudaGetLastError();
 }
@@ -721,17 +747,39 @@ cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallA
         default: { constexpr int NSV = 8; EXPR; } break;     \
     }
 
+// The context's FP32/FP64 pair split on a call's copy of the batch view: the near radius and the
+// rounding bands around the cutoffs (4e-6 rc^2, several times the largest FP32 error of a squared
+// distance up to the cutoff: entries and sites relative to a bin centre within rc plus a bin's
+// circumradius carry at most half an ulp of a coordinate below 16 Å each).
+void apply_split(const pa_context* ctx, pa::DevBatch<float>& v) {
+    const double rn = ctx->split.near_radius;
+    v.recip64 = ctx->split.fp64_reciprocal != 0 ? 1 : 0;
+    if (!(rn > 0)) {
+        v.rn2 = 0.f;
+        v.rl2_lo = v.rl2_hi = v.rl2;
+        v.re2_lo = v.re2_hi = v.re2;
+        return;
+    }
+    v.rn2 = float(rn * rn);
+    const double bl = 4.0e-6 * v.rl2_64, be = 4.0e-6 * v.re2_64;
+    v.rl2_lo = float(v.rl2_64 - bl); v.rl2_hi = float(v.rl2_64 + bl);
+    v.re2_lo = float(v.re2_64 - be); v.re2_hi = float(v.re2_64 + be);
+}
+
 template <typename F>
 pa_status set_pair_tables_impl(pa_context* ctx, pa_batch* B, const double* sigma, const double* epsilon,
                                const double* constant_offset) {
     const int N = B->nguest, nt = B->ntypes;
     std::vector<F> sig2(N * nt), eps4(N * nt);
+    std::vector<double> sig2_64(N * nt), eps4_64(N * nt);
     for (int a = 0; a < N; ++a) {
         const int gt = B->guest_types[a];
         for (int t = 0; t < nt; ++t) {
             const double sg = sigma[gt + nt * t], e = epsilon[gt + nt * t];
             sig2[a * nt + t] = F(sg * sg);
             eps4[a * nt + t] = F(4 * e);
+            sig2_64[a * nt + t] = sg * sg;
+            eps4_64[a * nt + t] = 4 * e;
             B->site_sigma[a * nt + t] = sg;
             B->site_eps[a * nt + t] = e;
         }
@@ -740,6 +788,10 @@ pa_status set_pair_tables_impl(pa_context* ctx, pa_batch* B, const double* sigma
     cudaStream_t st = ctx->stream;
     PA_CUDA(ctx, cudaMemcpyAsync(const_cast<F*>(d.sig2), sig2.data(), sizeof(F) * sig2.size(), cudaMemcpyHostToDevice, st));
     PA_CUDA(ctx, cudaMemcpyAsync(const_cast<F*>(d.eps4), eps4.data(), sizeof(F) * eps4.size(), cudaMemcpyHostToDevice, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(d.sig2_64), sig2_64.data(), sizeof(double) * sig2_64.size(),
+                                 cudaMemcpyHostToDevice, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(d.eps4_64), eps4_64.data(), sizeof(double) * eps4_64.size(),
+                                 cudaMemcpyHostToDevice, st));
     PA_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(d.const_offset), constant_offset, sizeof(double) * B->nfw,
                                  cudaMemcpyHostToDevice, st));
     return wait_stream(ctx);
@@ -823,6 +875,22 @@ pa_status pa_context_set_tuning(pa_context* ctx, const pa_tuning* t) {
         return fail(ctx, PA_ERR_ARG, "bin_width must be 0 or within [1, 50] Angstrom");
     if (t->ctas_per_sm < 0 || t->ctas_per_sm > PA_CTAS_PER_SM32) return fail(ctx, PA_ERR_ARG, "ctas_per_sm must be within [0, 8]");
     ctx->tuning = *t;
+    return PA_OK;
+}
+
+pa_status pa_context_set_fp32_split(pa_context* ctx, const pa_fp32_split* split) {
+    if (!ctx || !split) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (!(split->near_radius >= 0 && split->near_radius <= 100.0))
+        return fail(ctx, PA_ERR_ARG, "near_radius must be in [0, 100] Å");
+    if (split->fp64_reciprocal != 0 && split->fp64_reciprocal != 1)
+        return fail(ctx, PA_ERR_ARG, "fp64_reciprocal must be 0 or 1");
+    ctx->split = *split;
+    return PA_OK;
+}
+
+pa_status pa_context_get_fp32_split(const pa_context* ctx, pa_fp32_split* split) {
+    if (!ctx || !split) return PA_ERR_ARG;
+    *split = ctx->split;
     return PA_OK;
 }
 
@@ -1096,6 +1164,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     // table) and pose-independent terms replace the batch's, plus the live guests' sites
     pa::DevBatch<float> v32;  // byte copy (padding included: the bytes key the CUDA graph)
     std::memcpy(&v32, &B->d32, sizeof(v32));
+    apply_split(ctx, v32);
     pa::ChainArgs cargs{};
     int64_t ng = 0;
     if (chain) {
@@ -1776,8 +1845,11 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     {
         cudaError_t e = cudaSuccess;
         PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
-        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, B->d32, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
-        if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(B->d32, ca, w, ctx->num_sms, st))); }
+        pa::DevBatch<float> v32;  // the context's FP32/FP64 pair split, as pa_widom applies it
+        std::memcpy(&v32, &B->d32, sizeof(v32));
+        apply_split(ctx, v32);
+        if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, v32, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
+        if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(v32, ca, w, ctx->num_sms, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));
     }
     pa::k_segsum<<<unsigned(nseg), 256, 0, st>>>(w, args->kT, nullptr);

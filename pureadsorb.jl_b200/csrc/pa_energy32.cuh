@@ -34,6 +34,21 @@ __device__ __forceinline__ float ex2_ftz(float x) {
     return r;
 }
 
+// erfc(alpha r) / r in FP64 from r^2 and 1/r: 1/r - alpha S(alpha^2 r^2), S(u) = erf(sqrt u)/sqrt u
+// as a polynomial in u (PA_ERFS64, alpha r <= 2, relative error of erfc below 2e-13); CUDA's
+// double erfc beyond that.
+__device__ __forceinline__ double screened64(double r2, double ri, double alpha) {
+    const double u = (alpha * alpha) * r2;
+    if (u <= PA_ERFS64_UMAX) {
+        const double c[PA_NERFS64] = PA_ERFS64_INIT;
+        double p = c[PA_NERFS64 - 1];
+#pragma unroll
+        for (int k = PA_NERFS64 - 2; k >= 0; --k) p = fma(p, u, c[k]);
+        return fma(-alpha, p, ri);
+    }
+    return erfc(alpha * (r2 * ri)) * ri;
+}
+
 // Fetches the next tile of a persistent warp: its bin and the [lo, hi) range of sorted entries.
 __device__ __forceinline__ bool next_tile(const Work& w, int32_t nbins, int32_t lane, int32_t& bin, int32_t& lo,
                                           int32_t& hi) {
@@ -72,12 +87,18 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[PA_WARPS32][2];
     __shared__ float4 s_site[NS];    // body-frame site offsets, and the site charge times KE
+    __shared__ double4 s_site64[NS]; // the same in FP64 (the FP64 pairs)
+    __shared__ double2 s_p64[PA_WARPS32][32][2];  // each lane's site in FP64 (x, y | z, -), FP64 pairs
     extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int nt = b.ntypes;
     for (int x = tid; x < NS * nt; x += blockDim.x) { s_lj[x] = b.sig2[x]; s_lj[NS * nt + x] = b.eps4[x]; }
-    if (tid < NS) s_site[tid] = make_float4(b.gsite[3 * tid], b.gsite[3 * tid + 1], b.gsite[3 * tid + 2],
-                                            float(KE * double(b.gq[tid])));
+    if (tid < NS) {
+        s_site[tid] = make_float4(b.gsite[3 * tid], b.gsite[3 * tid + 1], b.gsite[3 * tid + 2],
+                                  float(KE * double(b.gq[tid])));
+        s_site64[tid] = make_double4(b.gsite64[3 * tid], b.gsite64[3 * tid + 1], b.gsite64[3 * tid + 2],
+                                     KE * b.gq64[tid]);
+    }
     if (lane == 0) { mbar_init(&s_bar[wp][0], 1); mbar_init(&s_bar[wp][1], 1); mbar_fence_init(); }
     __syncthreads();  // the only CTA-wide barrier: tables and barriers are ready
     const float* s_sig2 = s_lj;
@@ -108,9 +129,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         bin_centre(b, fw, bin, cx, cy, cz);
         const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
         const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
-        const float* A = b.cells + 9 * fw;
         const float* iA = b.invcells + 9 * fw;
-        // the site relative to the bin centre: A (rp + shift - c) + g
+        // the site relative to the bin centre, A (rp + shift - c) + g, in FP64 (the near pairs'
+        // geometry) and rounded once to FP32 for the rest; the lattice shift is the binning's own
         float px, py, pz;
         {
             const float q[4] = {pq.x, pq.y, pq.z, pq.w};
@@ -120,16 +141,30 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             rotate_s(q, gb, g);
             const float rp[3] = {pa.x, pa.y, pa.z};
             site_frac32(rp, g, iA, fs, sh);
-            // rp + shift - c is exact in FP64 (all three are FP32 values), then rounded once
-            const float d0 = float((double(pa.x) + double(sh[0])) - double(cx));
-            const float d1 = float((double(pa.y) + double(sh[1])) - double(cy));
-            const float d2 = float((double(pa.z) + double(sh[2])) - double(cz));
-            px = fmaf(A[6], d2, fmaf(A[3], d1, A[0] * d0)) + g[0];
-            py = fmaf(A[7], d2, fmaf(A[4], d1, A[1] * d0)) + g[1];
-            pz = fmaf(A[8], d2, fmaf(A[5], d1, A[2] * d0)) + g[2];
+            // rp + shift - c is exact in FP64 (all three are FP32 values)
+            const double d0 = (double(pa.x) + double(sh[0])) - double(cx);
+            const double d1 = (double(pa.y) + double(sh[1])) - double(cy);
+            const double d2 = (double(pa.z) + double(sh[2])) - double(cz);
+            const double qd[4] = {double(pq.x), double(pq.y), double(pq.z), double(pq.w)};
+            const double4 gs64 = s_site64[as];
+            const double gb64[3] = {gs64.x, gs64.y, gs64.z};
+            double g64[3];
+            rotate_s(qd, gb64, g64);
+            const double* A64 = b.cells64 + 9 * fw;
+            const double p64x = fma(A64[6], d2, fma(A64[3], d1, A64[0] * d0)) + g64[0];
+            const double p64y = fma(A64[7], d2, fma(A64[4], d1, A64[1] * d0)) + g64[1];
+            const double p64z = fma(A64[8], d2, fma(A64[5], d1, A64[2] * d0)) + g64[2];
+            s_p64[wp][lane][0] = make_double2(p64x, p64y);
+            s_p64[wp][lane][1] = make_double2(p64z, 0.0);
+            px = float(p64x); py = float(p64y); pz = float(p64z);
         }
         const float qk = s_site[as].w;
-        const float rl2 = b.rl2, re2 = b.re2, rc2 = fmaxf(rl2, re2), alpha = float(b.alphas[fw]);
+        const float rl2 = b.rl2, re2 = b.re2, alpha = float(b.alphas[fw]);
+        // FP32 distances below rc2 enter the pair block; of those, the near pairs and the ones in a
+        // cutoff's rounding band are evaluated in FP64
+        const float rc2 = fmaxf(b.rl2_hi, b.re2_hi), rn2 = b.rn2;
+        const float rl2lo = b.rl2_lo, rl2hi = b.rl2_hi, re2lo = b.re2_lo, re2hi = b.re2_hi;
+        double enear = 0.0;  // the FP64 pairs' sum
         const float NLOG2E = -1.4426950408889634f;
         const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
         const float halpha = 0.5f * alpha;
@@ -138,8 +173,8 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         // one type (the bin's run table), the same for every lane, so the loop runs uniformly from
         // one run boundary to the next and reloads them there
         const int2* runs = b.list_runs + int64_t(bin) * b.runs_per_bin;
-        int32_t ri = 0, rnext = runs[1].x;
-        float sg = s_sig2[as * nt + runs[0].y], ep = s_eps4[as * nt + runs[0].y];
+        int32_t ri = 0, rnext = runs[1].x, ty = runs[0].y;
+        float sg = s_sig2[as * nt + ty], ep = s_eps4[as * nt + ty];
         // without the adjoint sums: 4 eps ((sigma/r)^12 - (sigma/r)^6) = r^-6 (ljA r^-6 - ljB),
         // ljA = 4 eps sigma^12, ljB = 4 eps sigma^6, one multiplication fewer per pair
         float ljB = ep * (sg * sg * sg), ljA = ljB * (sg * sg * sg);
@@ -165,6 +200,26 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                         const float dx = px - at.x, dy = py - at.y, dz = pz - at.z;
                         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                         if (r2 < rc2) {
+                            // (with equal cutoffs r2 < rc2 = rl2hi already holds)
+                            if (r2 < rn2 || r2 > rl2lo && (EQCUT || r2 < rl2hi) || (!EQCUT && r2 > re2lo && r2 < re2hi)) {
+                                // a near pair, or one within a cutoff's rounding band: FP64 from the
+                                // FP64 entry and site, the cutoff tests, LJ and screened Coulomb
+                                const double4 e64 = b.list_xyzq64[base + j];
+                                const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
+                                const double ex = pxy.x - e64.x, ey = pxy.y - e64.y, ez = pzz.x - e64.z;
+                                const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
+                                const double rid = rsqrt(r2d);
+                                if (r2d < b.rl2_64) {
+                                    const double x = b.sig2_64[as * nt + ty] * (rid * rid);
+                                    const double x3 = x * x * x;
+                                    const double u = x3 * x3 - x3;
+                                    enear = fma(b.eps4_64[as * nt + ty], u, enear);
+                                    if (PQ) { sp += float(u); sq += float(fma(x3, x3, u)); }
+                                }
+                                if (charged && r2d < b.re2_64)
+                                    enear = fma(s_site64[as].w * e64.w, screened64(r2d, rid, b.alphas[fw]), enear);
+                                continue;
+                            }
                             float e = 0.f;
                             if (charged) {
                                 // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
@@ -193,7 +248,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                     for (int k = PA_NERFC32 - 2; k >= 0; --k) p = fmaf(p, tt, cf[k]);
                                     e = fmaf(qk * at.w, p * ex2_ftz(r2 * a2n) * ri, e);
                                 }
-                            } else {
+                            } else if (EQCUT || r2 < rl2) {
                                 if (PQ) {
                                     const float x = sg * rcp_nr(r2);
                                     const float x3 = x * x * x;
@@ -217,7 +272,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                         sp = 0.f; sq = 0.f;
                     }
                     ++ri;
-                    const int32_t ty = runs[ri].y;
+                    ty = runs[ri].y;
                     rnext = runs[ri + 1].x;
                     sg = s_sig2[as * nt + ty];
                     ep = s_eps4[as * nt + ty];
@@ -239,7 +294,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             return;
         }
         if (PQ && active && nch > 0) runsums[ri] = make_float2(sp, sq);  // the last run
-        if (active) w.dUs[it] = double(esum) - double(ecmp);
+        if (active) w.dUs[it] = (double(esum) - double(ecmp)) + enear;
     }
 }
 
@@ -338,5 +393,91 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
         }
         kahan_add(acc, cacc, row);
         if (active) w.dUr[li] = KE * (double(acc) - double(cacc));
+    }
+}
+
+// The reciprocal cross term in FP64 (the FP32 path's accurate form): the same tiles and row
+// recurrences as k_recip32, with the sites' fractional offsets from the bin centre, the phase
+// factors, the row starts (FP64 sincospi of the phase reduced to half a turn), the recurrences and
+// the sums all in FP64. Writes KE E_lr.
+template <int NS>
+__global__ void __launch_bounds__(32 * PA_WARPS32) k_recip64(DevBatch<float> b, CallArgs ca, Work w) {
+    __shared__ double2 s_B[PA_WARPS32][PA_KCHUNK32];
+    __shared__ float4 s_kc[PA_WARPS32][PA_KCHUNK32];
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    int32_t bin = 0, lo = 0, hi = 0;
+    while (next_tile(w, b.nbins, lane, bin, lo, hi)) {
+        const int32_t fw = b.bin_fw[bin];
+        const bool active = lo + lane < hi;
+        const int32_t li = active ? w.sorted[lo + lane] : 0;
+        float cx, cy, cz;
+        bin_centre(b, fw, bin, cx, cy, cz);
+        const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
+        const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
+        const double* iA = b.invcells64 + 9 * fw;
+        const double d0 = double(pa.x) - double(cx), d1 = double(pa.y) - double(cy), d2 = double(pa.z) - double(cz);
+        double dfr[3 * NS];
+        {
+            const double q[4] = {double(pq.x), double(pq.y), double(pq.z), double(pq.w)};
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const double gb[3] = {b.gsite64[3 * s], b.gsite64[3 * s + 1], b.gsite64[3 * s + 2]};
+                double g[3];
+                rotate_s(q, gb, g);
+                dfr[3 * s + 0] = d0 + fma(iA[6], g[2], fma(iA[3], g[1], iA[0] * g[0]));
+                dfr[3 * s + 1] = d1 + fma(iA[7], g[2], fma(iA[4], g[1], iA[1] * g[0]));
+                dfr[3 * s + 2] = d2 + fma(iA[8], g[2], fma(iA[5], g[1], iA[2] * g[0]));
+            }
+        }
+        const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
+        double stc[NS], sts[NS], cr[NS], ci[NS];
+        const double kst = double(b.kstep[fw]);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            sincospi(2.0 * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
+            cr[s] = 1.0; ci[s] = 0.0;
+        }
+        double acc = 0.0;
+        for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
+            const int32_t kn = min(PA_KCHUNK32, k1 - kb);
+            for (int32_t x = lane; x < kn; x += 32) {
+                const int32_t kk = kb + x;
+                const float4 kc = b.kcoef4[kk];
+                s_kc[wp][x] = kc;
+                double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
+                ph -= rint(ph);
+                double sn, cs;
+                sincospi(2.0 * ph, &sn, &cs);
+                const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
+                s_B[wp][x] = make_double2(Sr * cs + Si * sn, Sr * sn - Si * cs);
+            }
+            __syncwarp();
+            for (int32_t x = 0; x < kn; ++x) {
+                const float4 kc = s_kc[wp][x];
+                if (kc.w == 0.f) {  // row start: direct evaluation
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        double ph = fma(double(kc.z), dfr[3 * s + 2], fma(double(kc.y), dfr[3 * s + 1],
+                                                                          double(kc.x) * dfr[3 * s]));
+                        ph -= rint(ph);
+                        sincospi(2.0 * ph, &ci[s], &cr[s]);
+                    }
+                } else {  // next k-vector of the row
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const double r = fma(cr[s], stc[s], -ci[s] * sts[s]);
+                        ci[s] = fma(cr[s], sts[s], ci[s] * stc[s]);
+                        cr[s] = r;
+                    }
+                }
+                double gr = 0.0, gi = 0.0;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) { gr = fma(b.gq64[s], cr[s], gr); gi = fma(b.gq64[s], ci[s], gi); }
+                const double2 B = s_B[wp][x];
+                acc = fma(B.x, gr, fma(-B.y, gi, acc));
+            }
+            __syncwarp();
+        }
+        if (active) w.dUr[li] = KE * acc;
     }
 }

@@ -65,6 +65,19 @@ struct DevBatch {
     const int2* list_runs;                        // nbins*runs_per_bin: each bin's type runs (first entry,
                                                   // type), then (end of the list, 0) up to runs_per_bin
     int32_t runs_per_bin;
+    // FP32 path, pairs evaluated in FP64: those closer than the near radius and those whose FP32
+    // distance lies within a rounding band of a cutoff (the band's edges, rl2/re2 -+ band)
+    const double4* list_xyzq64;                   // the list entries in FP64 (position, charge)
+    const double* cells64;                        // 9*nfw
+    const double* invcells64;                     // 9*nfw
+    const double* sig2_64;                        // nguest*ntypes
+    const double* eps4_64;                        // nguest*ntypes
+    double gsite64[3 * PA_MAX_SITES_DEV];
+    double gq64[PA_MAX_SITES_DEV];
+    double rl2_64, re2_64;                        // the cutoffs squared, FP64
+    F rn2;                                        // near radius squared (0: no near pairs)
+    int32_t recip64;                              // 1: the reciprocal term in FP64 (k_recip64)
+    F rl2_lo, rl2_hi, re2_lo, re2_hi;             // rounding bands around the cutoffs
 };
 
 // Per-call arguments shared by the kernels.
@@ -1027,6 +1040,7 @@ struct ListGeom {
     int32_t* counts;           // nbins (count pass)
     const int32_t* offsets;    // nbins+1 (fill pass)
     float4* xyzq;
+    double4* xyzq64;           // the same entries in FP64
     int32_t* type_out;
     int32_t* atom_out;         // stored-atom index of each entry (for the adjoint)
 };
@@ -1168,6 +1182,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
                                 const double dy = dot3s(A[1], A[4], A[7], d0, d1, d2);
                                 const double dz = dot3s(A[2], A[5], A[8], d0, d1, d2);
                                 g.xyzq[pos] = make_float4(float(dx), float(dy), float(dz), qa);
+                                g.xyzq64[pos] = make_double4(dx, dy, dz, g.charges[ja]);
                                 g.type_out[pos] = ta;
                                 g.atom_out[pos] = ja;
                             }
@@ -1194,6 +1209,7 @@ __global__ void __launch_bounds__(256) k_lists(ListGeom g) {
         const int32_t end = g.offsets[bin + 1];
         for (int32_t q = s_base + threadIdx.x; q < end; q += blockDim.x) {
             g.xyzq[q] = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.0f);
+            g.xyzq64[q] = make_double4(1.0e15, 1.0e15, 1.0e15, 0.0);
             g.type_out[q] = 0;
             g.atom_out[q] = 0;
         }

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from test_chain import chain_view, small_charged
-from test_gpu_parity import F32_ABS, F32_REL
+from test_gpu_parity import FAST_ABS, FAST_REL
 
 pytestmark = pytest.mark.gpu
 
@@ -54,7 +54,7 @@ def _device_vs_oracle(pa, orc, b, st, guest, ff, ins, kT):
         dev = ins["dU"][sl]
         fin = np.isfinite(ref) & (ref < 50.0)  # the weight of larger ΔU is exp(-1900) or less
         err = np.abs(dev[fin] - ref[fin])
-        tol = F32_ABS + F32_REL * np.abs(ref[fin])
+        tol = FAST_ABS + FAST_REL * np.abs(ref[fin])  # the guest-guest term is FP32
         bad += int(np.sum(err > tol))
         n += int(fin.sum())
         assert np.all(err <= 2 * tol), (s, np.max(err / tol))

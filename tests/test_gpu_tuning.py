@@ -5,7 +5,7 @@ the FP32 tolerance of the parity tests; the autotuner leaves its choice set on t
 import numpy as np
 import pytest
 
-from test_gpu_parity import F32_ABS, F32_REL
+from test_gpu_parity import within_f32
 
 pytestmark = pytest.mark.gpu
 
@@ -76,7 +76,7 @@ def test_bin_width_and_grid_keep_results(pa, co2_batch, width, ctas):
     assert np.array_equal(ins["flags"], ref["flags"])
     surv = ref["flags"] == 0
     a, b = ins["dU"][surv], ref["dU"][surv]
-    assert np.all(np.abs(a - b) <= 2 * (F32_ABS + F32_REL * np.abs(b)))
+    assert np.all(within_f32(a, b))
 
 
 def test_autotune_sets_its_choice(pa, co2_batch):
