@@ -25,6 +25,11 @@ constexpr int NCLASS = 8;  // kernel classes: pose, scan/scatter, energy, reduce
                            // guest-guest
 constexpr double LIST_PAD = 32;
 constexpr double DEFAULT_BIN_WIDTH = 3.0;  // Angstrom, FP32 path spatial bins
+// The FP32 path's split k tables: the k-vectors of largest |k| go to FP32 rows while
+// KE sqrt(Σ |2 kpref S_k|^2) Σ|q_guest| KSPLIT_EPS32 stays within KSPLIT_BUDGET (eV), KSPLIT_EPS32
+// bounding the FP32 error of G_k per unit guest charge (phases, row starts, recurrences)
+constexpr double KSPLIT_EPS32 = 1.0e-6;
+constexpr double KSPLIT_BUDGET = 3.0e-9;
 constexpr double WAIT_LIMIT_S = 600.0;      // host-side bound on one call's device work
 
 struct DevMem {
@@ -75,7 +80,8 @@ struct pa_context {
     bool want_pq = false;
     DevMem item_pq;
     // insertion into a loaded configuration: per-call tables and the guest-guest term
-    DevMem chain_kS2, chain_const, chain_goff, chain_gsites, chain_gtype, chain_cells, dUg;
+    DevMem chain_kS2, chain_const, chain_goff, chain_gsites, chain_gtype, chain_cells, dUg, chain_ksplit;
+    std::vector<unsigned char> up_chain_ksplit;
     std::vector<double> up_chain_kS2, up_chain_const, up_chain_gsites, up_chain_cells;
     std::vector<int32_t> up_chain_goff, up_chain_gtype;
     // launch choices, the replayable graph of the last call's device sequence and its key
@@ -133,6 +139,11 @@ struct pa_batch {
     std::vector<int32_t> guest_types;  // 0-based compact type of each guest site
     std::vector<double> guest_q;       // guest site charges
     std::vector<double> recip_bound;   // per framework Σ_k kpref |S_k| (hard-core bound)
+    // the k tables' host copies the split tables are built from (FP32 path, charged guest)
+    std::vector<double> kvec_h;        // 3*nk Cartesian k
+    std::vector<int32_t> kn_h;         // 3*nk integer coefficients
+    std::vector<int32_t> kstep_h;      // nfw: row step in n3
+    double guest_qabs = 0;             // Σ |guest charge|
     double cutoff = 0;                 // LJ cutoff
     const double* q64 = nullptr;       // FP64 charges of the stored atoms (inside the arena)
     const int32_t* types0 = nullptr;   // 0-based types (inside the arena)
@@ -345,6 +356,8 @@ struct Slots {
         cellgrid_offsets, k_offsets, kvec, kcoef, kstep, kS2, kpref2, sig2, eps4, bin_dims, bin_base, bin_fw;
     size_t list_offsets, list_xyzq, list_type, list_atom, list_runs, list_xyzq64;  // inside the list allocation
     size_t cells64, invcells64, sig2_64, eps4_64;
+    size_t ks64_coef, ks64_S2, ks64_off, ks32_coef, ks32_S2, ks32_off;
+    bool ksplit;
 };
 
 template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, const pa_batch_desc* desc, const Slots& o) {
@@ -399,9 +412,67 @@ template <typename F> void fill_batch_view(pa_batch* B, pa::DevBatch<F>& d, cons
     d.rl2_64 = desc->cutoff * desc->cutoff;
     d.re2_64 = desc->ewald_cutoff * desc->ewald_cutoff;
     d.rn2 = F(0);  // set per call from the context's split
-    d.recip64 = 0;
+    d.rmode = 0;
+    d.has_ksplit = o.ksplit ? 1 : 0;
+    d.ks64_coef = reinterpret_cast<const float4*>(a + o.ks64_coef);
+    d.ks64_S2 = reinterpret_cast<const double*>(a + o.ks64_S2);
+    d.ks64_off = reinterpret_cast<const int32_t*>(a + o.ks64_off);
+    d.ks32_coef = reinterpret_cast<const float4*>(a + o.ks32_coef);
+    d.ks32_S2 = reinterpret_cast<const double*>(a + o.ks32_S2);
+    d.ks32_off = reinterpret_cast<const int32_t*>(a + o.ks32_off);
     d.rl2_lo = d.rl2_hi = d.rl2;
     d.re2_lo = d.re2_hi = d.re2;
+}
+
+// The FP32 path's split k tables from 2 kpref S per k-vector: per framework, the k-vectors of largest
+// |k| go to the FP32 set while KE sqrt(Σ |2 kpref S_k|^2) Σ|q_guest| KSPLIT_EPS32 <= KSPLIT_BUDGET (ties
+// by enumeration index), the rest to the FP64 set; each set in enumeration order, a row continuing
+// only over consecutive members of its set. Packed as one byte image with its slot offsets.
+struct KSplit {
+    std::vector<float4> c64, c32;
+    std::vector<double> s64, s32;
+    std::vector<int32_t> o64{0}, o32{0};
+};
+KSplit build_ksplit(const pa_batch* B, const double* kS2) {
+    KSplit r;
+    for (int fw = 0; fw < B->nfw; ++fw) {
+        const int32_t k0 = B->k_offsets[fw], k1 = B->k_offsets[fw + 1], step = B->kstep_h[fw];
+        const int32_t* n = B->kn_h.data() + 3 * int64_t(k0);
+        std::vector<int32_t> ord(k1 - k0);
+        for (int32_t q = 0; q < k1 - k0; ++q) ord[q] = q;
+        const auto k2 = [&](int32_t q) {
+            const double* v = &B->kvec_h[3 * int64_t(k0 + q)];
+            return v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        };
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t c) { return k2(a) > k2(c); });
+        std::vector<char> f32k(k1 - k0, 0);
+        double sum = 0;
+        for (int32_t q : ord) {
+            const double bx = kS2[2 * (k0 + q)], by = kS2[2 * (k0 + q) + 1];
+            sum += bx * bx + by * by;
+            if (pa::KE * std::sqrt(sum) * B->guest_qabs * KSPLIT_EPS32 > KSPLIT_BUDGET) break;
+            f32k[q] = 1;
+        }
+        for (int part = 0; part < 2; ++part) {
+            std::vector<float4>& co = part ? r.c32 : r.c64;
+            std::vector<double>& sv = part ? r.s32 : r.s64;
+            int32_t prev = -1;
+            for (int32_t q = 0; q < k1 - k0; ++q) {
+                if (f32k[q] != part) continue;
+                const bool cont = prev >= 0 && n[3 * q] == n[3 * prev] && n[3 * q + 1] == n[3 * prev + 1] &&
+                                  n[3 * q + 2] - n[3 * prev + 2] == step;
+                co.push_back(make_float4(float(n[3 * q]), float(n[3 * q + 1]), float(n[3 * q + 2]), cont ? 1.f : 0.f));
+                sv.push_back(kS2[2 * (k0 + q)]);
+                sv.push_back(kS2[2 * (k0 + q) + 1]);
+                prev = q;
+            }
+            (part ? r.o32 : r.o64).push_back(int32_t(co.size()));
+        }
+    }
+    // never empty (the device pointers stay valid)
+    if (r.c64.empty()) { r.c64.push_back(make_float4(0, 0, 0, 0)); r.s64.resize(2, 0.0); }
+    if (r.c32.empty()) { r.c32.push_back(make_float4(0, 0, 0, 0)); r.s32.resize(2, 0.0); }
+    return r;
 }
 
 template <typename F>
@@ -532,6 +603,15 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     std::vector<double> kvec(desc->ks, desc->ks + 3 * nk), kS2(2 * nk), kpref2(nk);
     std::vector<float4> kcoef4(nk);
     std::vector<float> kstep(nfw, 1.0f);
+    double qg = 0;
+    for (int a = 0; a < N; ++a) qg += std::fabs(desc->guest_charges[a]);
+    const bool ksplit = sizeof(F) == 4 && qg > 0;
+    if (ksplit) {
+        B->kvec_h = kvec;
+        B->kn_h.assign(3 * nk, 0);
+        B->kstep_h.assign(nfw, 1);
+        B->guest_qabs = qg;
+    }
     for (int64_t i = 0; i < nk; ++i) {
         kS2[2 * i] = 2 * desc->kprefactor[i] * desc->Shost[2 * i];
         kS2[2 * i + 1] = 2 * desc->kprefactor[i] * desc->Shost[2 * i + 1];
@@ -561,6 +641,11 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
             bool cont = q > 0 && n[3 * q] == n[3 * q - 3] && n[3 * q + 1] == n[3 * q - 2] &&
                         n[3 * q + 2] - n[3 * q - 1] == step;
             kcoef4[k0 + q] = make_float4(float(n[3 * q]), float(n[3 * q + 1]), float(n[3 * q + 2]), cont ? 1.f : 0.f);
+        }
+        if (ksplit) {
+            for (int32_t q = 0; q < k1 - k0; ++q)
+                for (int r = 0; r < 3; ++r) B->kn_h[3 * int64_t(k0 + q) + r] = n[3 * q + r];
+            B->kstep_h[fw] = step;
         }
     }
     std::vector<F> sig2(N * nt), eps4(N * nt);
@@ -595,6 +680,12 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     o.cells64 = pk.add(std::vector<double>(desc->cells, desc->cells + 9 * nfw));
     o.invcells64 = pk.add(std::vector<double>(desc->invcells, desc->invcells + 9 * nfw));
     o.sig2_64 = pk.add(sig2_64); o.eps4_64 = pk.add(eps4_64);
+    o.ksplit = ksplit;
+    if (ksplit) {
+        const KSplit ks = build_ksplit(B, kS2.data());
+        o.ks64_coef = pk.add(ks.c64); o.ks64_S2 = pk.add(ks.s64); o.ks64_off = pk.add(ks.o64);
+        o.ks32_coef = pk.add(ks.c32); o.ks32_S2 = pk.add(ks.s32); o.ks32_off = pk.add(ks.o32);
+    }
     if (lists) { t_order = pk.add(order); t_frac = pk.add(frac); }
     if (!pk.ok) return fail(ctx, PA_ERR_CUDA, "pinned staging allocation failed");
     PA_CUDA(ctx, cudaMallocAsync(&B->arena, pk.n, st));
@@ -729,8 +820,11 @@ cudaError_t launch_grad(const pa_batch* B, const pa::CallArgs& ca, const pa::Wor
 template <int NS>
 cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallArgs& ca, const pa::Work& w,
                                  int32_t num_sms, cudaStream_t st) {
-    if (v32.has_charge && v32.recip64) pa::k_recip64<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
-    else if (v32.has_charge) pa::k_recip32<NS><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+    if (v32.has_charge) {
+        if (v32.rmode == 2) pa::k_recip<NS, 2><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+        else if (v32.rmode == 1) pa::k_recip<NS, 1><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+        else pa::k_recip<NS, 0><<<num_sms * 8, 32 * PA_WARPS32, 0, st>>>(v32, ca, w);
+    }
     pa::k_combine<NS><<<unsigned((ca.n_act + 255) / 256), 256, 0, st>>>(v32, ca, w);
     return cudaGetLastError();
 }
@@ -753,7 +847,7 @@ cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallA
 // circumradius carry at most half an ulp of a coordinate below 16 Å each).
 void apply_split(const pa_context* ctx, pa::DevBatch<float>& v) {
     const double rn = ctx->split.near_radius;
-    v.recip64 = ctx->split.fp64_reciprocal != 0 ? 1 : 0;
+    v.rmode = ctx->split.fp64_reciprocal == 0 ? 0 : v.has_ksplit ? 2 : 1;
     if (!(rn > 0)) {
         v.rn2 = 0.f;
         v.rl2_lo = v.rl2_hi = v.rl2;
@@ -1189,6 +1283,29 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
         PA_CUDA(ctx, upload_cached(ctx->chain_cells, ctx->up_chain_cells, cl, st));
         PA_CUDA(ctx, ctx->dUg.ensure(sizeof(double) * n_act));
         v32.kS2 = ctx->chain_kS2.as<double>();
+        if (v32.rmode == 2) {
+            // the split tables of the running S(k), one packed upload
+            const KSplit ks = build_ksplit(B, ks2.data());
+            const auto up8 = [](size_t x) { return (x + 255) & ~size_t(255); };
+            const size_t o1 = 0, o2 = up8(o1 + 16 * ks.c64.size()), o3 = up8(o2 + 8 * ks.s64.size()),
+                         o4 = up8(o3 + 4 * ks.o64.size()), o5 = up8(o4 + 16 * ks.c32.size()),
+                         o6 = up8(o5 + 8 * ks.s32.size()), oend = o6 + 4 * ks.o32.size();
+            std::vector<unsigned char> img(oend, 0);
+            std::memcpy(img.data() + o1, ks.c64.data(), 16 * ks.c64.size());
+            std::memcpy(img.data() + o2, ks.s64.data(), 8 * ks.s64.size());
+            std::memcpy(img.data() + o3, ks.o64.data(), 4 * ks.o64.size());
+            std::memcpy(img.data() + o4, ks.c32.data(), 16 * ks.c32.size());
+            std::memcpy(img.data() + o5, ks.s32.data(), 8 * ks.s32.size());
+            std::memcpy(img.data() + o6, ks.o32.data(), 4 * ks.o32.size());
+            PA_CUDA(ctx, upload_cached(ctx->chain_ksplit, ctx->up_chain_ksplit, img, st));
+            const char* kb = static_cast<const char*>(ctx->chain_ksplit.p);
+            v32.ks64_coef = reinterpret_cast<const float4*>(kb + o1);
+            v32.ks64_S2 = reinterpret_cast<const double*>(kb + o2);
+            v32.ks64_off = reinterpret_cast<const int32_t*>(kb + o3);
+            v32.ks32_coef = reinterpret_cast<const float4*>(kb + o4);
+            v32.ks32_S2 = reinterpret_cast<const double*>(kb + o5);
+            v32.ks32_off = reinterpret_cast<const int32_t*>(kb + o6);
+        }
         v32.const_offset = ctx->chain_const.as<double>();
         cargs.gsites = ctx->chain_gsites.as<double>();
         cargs.goff = ctx->chain_goff.as<int32_t>();

@@ -80,6 +80,30 @@ __device__ __forceinline__ void bin_centre(const DevBatch<float>& b, int32_t fw,
     cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
 }
 
+// One pair in FP64 from the FP64 list entry e and the item's FP64 site (relative to the bin
+// centre): the cutoff tests, LJ and the screened Coulomb term (skq = KE times the site charge),
+// added to enear; PQ also adds the pair's x^6(x^6-1) and x^6(2x^6-1) (x = sigma/r) to the run sums.
+template <bool PQ>
+__device__ __forceinline__ void pair64(const DevBatch<float>& b, int32_t e, double px, double py, double pz,
+                                       int32_t as, int32_t ty, double skq, int32_t fw, bool charged, double& enear,
+                                       float& sp, float& sq) {
+    const double4 e64 = b.list_xyzq64[e];
+    const double ex = px - e64.x, ey = py - e64.y, ez = pz - e64.z;
+    const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
+    const double rid = rsqrt(r2d);
+    const int32_t nt = b.ntypes;
+    double en = 0.0;
+    if (r2d < b.rl2_64) {
+        const double x = b.sig2_64[as * nt + ty] * (rid * rid);
+        const double x3 = x * x * x;
+        const double u = x3 * x3 - x3;
+        en = b.eps4_64[as * nt + ty] * u;
+        if (PQ) { sp += float(u); sq += float(fma(x3, x3, u)); }
+    }
+    if (charged && r2d < b.re2_64) en = fma(skq * e64.w, screened64(r2d, rid, b.alphas[fw]), en);
+    enear += en;
+}
+
 // EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms. PQ: also store each
 // item's LJ sums per type run (w.item_pq) for the adjoint.
 template <int NS, bool EQCUT, bool PQ>
@@ -89,6 +113,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     __shared__ float4 s_site[NS];    // body-frame site offsets, and the site charge times KE
     __shared__ double4 s_site64[NS]; // the same in FP64 (the FP64 pairs)
     __shared__ double2 s_p64[PA_WARPS32][32][2];  // each lane's site in FP64 (x, y | z, -), FP64 pairs
+    __shared__ uint32_t s_mk[PA_WARPS32][PA_CHUNK32 / 32][32];  // per lane: the chunk's FP64 entries (bits)
     extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int nt = b.ntypes;
@@ -191,6 +216,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             const int32_t n = min(PA_CHUNK32, l1 - (l0 + c * PA_CHUNK32));
             if (tmo_at < 0) {
                 const int32_t base = l0 + c * PA_CHUNK32;
+                // the chunk's entries this lane evaluates in FP64 afterwards (bit j % 32 of word j / 32)
+#pragma unroll
+                for (int q = 0; q < PA_CHUNK32 / 32; ++q) s_mk[wp][q][lane] = 0u;
                 int32_t j = 0;
                 for (;;) {
                     const int32_t jend = min(n, rnext - base);
@@ -202,22 +230,15 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                         if (r2 < rc2) {
                             // (with equal cutoffs r2 < rc2 = rl2hi already holds)
                             if (r2 < rn2 || r2 > rl2lo && (EQCUT || r2 < rl2hi) || (!EQCUT && r2 > re2lo && r2 < re2hi)) {
-                                // a near pair, or one within a cutoff's rounding band: FP64 from the
-                                // FP64 entry and site, the cutoff tests, LJ and screened Coulomb
-                                const double4 e64 = b.list_xyzq64[base + j];
-                                const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
-                                const double ex = pxy.x - e64.x, ey = pxy.y - e64.y, ez = pzz.x - e64.z;
-                                const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
-                                const double rid = rsqrt(r2d);
-                                if (r2d < b.rl2_64) {
-                                    const double x = b.sig2_64[as * nt + ty] * (rid * rid);
-                                    const double x3 = x * x * x;
-                                    const double u = x3 * x3 - x3;
-                                    enear = fma(b.eps4_64[as * nt + ty], u, enear);
-                                    if (PQ) { sp += float(u); sq += float(fma(x3, x3, u)); }
+                                // a near pair, or one within a cutoff's rounding band: evaluated in
+                                // FP64 (the adjoint's form here, every other form after the chunk)
+                                if (PQ) {
+                                    const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
+                                    pair64<true>(b, base + j, pxy.x, pxy.y, pzz.x, as, ty, s_site64[as].w, fw, charged,
+                                                 enear, sp, sq);
+                                } else {
+                                    s_mk[wp][j >> 5][lane] |= 1u << (j & 31);
                                 }
-                                if (charged && r2d < b.re2_64)
-                                    enear = fma(s_site64[as].w * e64.w, screened64(r2d, rid, b.alphas[fw]), enear);
                                 continue;
                             }
                             float e = 0.f;
@@ -279,6 +300,24 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                     ljB = ep * (sg * sg * sg);
                     ljA = ljB * (sg * sg * sg);
                 }
+                if (!PQ) {
+                    // the marked pairs in FP64, lanes in step (each takes its next marked entry)
+                    const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
+                    const double skq = s_site64[as].w;
+                    float dsp = 0.f, dsq = 0.f;
+#pragma unroll 1
+                    for (int32_t q = 0; q < PA_CHUNK32 / 32; ++q) {
+                        uint32_t mq = s_mk[wp][q][lane];
+                        while (__any_sync(FULL, mq != 0)) {
+                            if (mq != 0) {
+                                const int32_t e = base + q * 32 + __ffs(mq) - 1;
+                                mq &= mq - 1;
+                                pair64<false>(b, e, pxy.x, pxy.y, pzz.x, as, b.list_type[e], skq, fw, charged, enear,
+                                              dsp, dsq);
+                            }
+                        }
+                    }
+                }
             }
             __syncwarp();  // the warp is done with stage st
             if (lane == 0 && tmo_at < 0 && c + 2 < nch) {
@@ -303,17 +342,132 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
 // the bin centre. Along a row of equal (n1, n2), n3 advances by the framework's step, so
 // e^{2 pi i n.d_s} is carried by one complex multiplication and evaluated directly only at row
 // starts. Tiles of 32 insertions of one bin (insertion order, not site order); writes KE E_lr.
+//
+// Three forms (RMODE): 0 every k-vector in FP32 (row starts from the hardware sine and cosine of the
+// phase reduced to half a turn, FP32 recurrences, rows compensated); 1 every k-vector in FP64
+// (sincospi row starts, FP64 recurrences and sums); 2 the batch's split tables: the k-vectors of
+// small |k| (the large terms) in FP64, the rest in FP32, chosen at upload so that the FP32 part's
+// rounding stays below a few 1e-9 eV.
+
+// The FP64 rows of one table [k0, k1): Σ_k Re(B_k G_k) in FP64.
 template <int NS>
-__global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, CallArgs ca, Work w) {
-    __shared__ float2 s_B[PA_WARPS32][PA_KCHUNK32];
+__device__ __forceinline__ double rows64(const float4* kcoef, const double* kS2, int32_t k0, int32_t k1,
+                                         const double* dfr, const double* stc, const double* sts, const double* gq,
+                                         float cx, float cy, float cz, int lane, double2* sB, float4* sKc) {
+    double cr[NS], ci[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) { cr[s] = 1.0; ci[s] = 0.0; }
+    double acc = 0.0;
+    for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
+        const int32_t kn = min(PA_KCHUNK32, k1 - kb);
+        for (int32_t x = lane; x < kn; x += 32) {
+            const int32_t kk = kb + x;
+            const float4 kc = kcoef[kk];
+            sKc[x] = kc;
+            double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
+            ph -= rint(ph);
+            double sn, cs;
+            sincospi(2.0 * ph, &sn, &cs);
+            const double Sr = kS2[2 * kk], Si = kS2[2 * kk + 1];
+            sB[x] = make_double2(Sr * cs + Si * sn, Sr * sn - Si * cs);
+        }
+        __syncwarp();
+        for (int32_t x = 0; x < kn; ++x) {
+            const float4 kc = sKc[x];
+            if (kc.w == 0.f) {  // row start: direct evaluation
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double ph = fma(double(kc.z), dfr[3 * s + 2], fma(double(kc.y), dfr[3 * s + 1], double(kc.x) * dfr[3 * s]));
+                    ph -= rint(ph);
+                    sincospi(2.0 * ph, &ci[s], &cr[s]);
+                }
+            } else {  // next k-vector of the row
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const double r = fma(cr[s], stc[s], -ci[s] * sts[s]);
+                    ci[s] = fma(cr[s], sts[s], ci[s] * stc[s]);
+                    cr[s] = r;
+                }
+            }
+            double gr = 0.0, gi = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) { gr = fma(gq[s], cr[s], gr); gi = fma(gq[s], ci[s], gi); }
+            const double2 B = sB[x];
+            acc = fma(B.x, gr, fma(-B.y, gi, acc));
+        }
+        __syncwarp();
+    }
+    return acc;
+}
+
+// The FP32 rows of one table [k0, k1): Σ_k Re(B_k G_k) as a compensated sum of row sums (acc, cacc).
+template <int NS>
+__device__ __forceinline__ void rows32(const float4* kcoef, const double* kS2, int32_t k0, int32_t k1,
+                                       const float* dfr, const float* stc, const float* sts, const float* gqs,
+                                       float cx, float cy, float cz, int lane, float2* sB, float4* sKc, float& acc,
+                                       float& cacc) {
+    float cr[NS], ci[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) { cr[s] = 1.f; ci[s] = 0.f; }
+    // the terms of one k-vector row (a few) are summed plainly, rows then compensated
+    float row = 0.f;
+    for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
+        const int32_t kn = min(PA_KCHUNK32, k1 - kb);
+        for (int32_t x = lane; x < kn; x += 32) {
+            const int32_t kk = kb + x;
+            const float4 kc = kcoef[kk];
+            sKc[x] = kc;
+            double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
+            ph -= rint(ph);
+            double sn, cs;
+            sincospi(2.0 * ph, &sn, &cs);
+            const double Sr = kS2[2 * kk], Si = kS2[2 * kk + 1];
+            // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
+            sB[x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
+        }
+        __syncwarp();
+        for (int32_t x = 0; x < kn; ++x) {
+            const float4 kc = sKc[x];
+            if (kc.w == 0.f) {  // row start: direct evaluation; the finished row enters the sum
+                kahan_add(acc, cacc, row);
+                row = 0.f;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    // the phase reduced to [-1/2, 1/2] turns, then the hardware sine and
+                    // cosine (absolute error about 4e-7 on [-pi, pi])
+                    float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
+                    ph -= rintf(ph);
+                    __sincosf(6.28318530717958648f * ph, &ci[s], &cr[s]);
+                }
+            } else {  // next k-vector of the row
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
+                    ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
+                    cr[s] = r;
+                }
+            }
+            float gr = 0.f, gi = 0.f;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
+            const float2 B = sB[x];
+            row = fmaf(B.x, gr, fmaf(-B.y, gi, row));
+        }
+        __syncwarp();
+    }
+    kahan_add(acc, cacc, row);
+}
+
+template <int NS, int RMODE>
+__global__ void __launch_bounds__(32 * PA_WARPS32) k_recip(DevBatch<float> b, CallArgs ca, Work w) {
+    __shared__ double2 s_B64[PA_WARPS32][PA_KCHUNK32];
+    __shared__ float2 s_B32[PA_WARPS32][PA_KCHUNK32];
     __shared__ float4 s_kc[PA_WARPS32][PA_KCHUNK32];
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    float gqs[NS], gsb[3 * NS];
+    double gq64[NS];
+    float gq32[NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        gqs[s] = b.gq[s];
-        gsb[3 * s] = b.gsite[3 * s]; gsb[3 * s + 1] = b.gsite[3 * s + 1]; gsb[3 * s + 2] = b.gsite[3 * s + 2];
-    }
+    for (int s = 0; s < NS; ++s) { gq64[s] = b.gq64[s]; gq32[s] = b.gq[s]; }
     int32_t bin = 0, lo = 0, hi = 0;
     while (next_tile(w, b.nbins, lane, bin, lo, hi)) {
         const int32_t fw = b.bin_fw[bin];
@@ -323,102 +477,35 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip32(DevBatch<float> b, 
         bin_centre(b, fw, bin, cx, cy, cz);
         const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
         const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
-        const float* iA = b.invcells + 9 * fw;
-        const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
-        float dfr[3 * NS];
-        {
+        double E = 0.0;
+        if (RMODE == 0) {
+            // FP32 site offsets from the bin centre and FP32 rows over the whole table
+            const float* iA = b.invcells + 9 * fw;
+            const float d0 = pa.x - cx, d1 = pa.y - cy, d2 = pa.z - cz;
+            float dfr[3 * NS], stc[NS], sts[NS];
             const float q[4] = {pq.x, pq.y, pq.z, pq.w};
+            const float kst = b.kstep[fw];
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 float g[3];
-                rotate_s(q, gsb + 3 * s, g);
+                const float gb[3] = {b.gsite[3 * s], b.gsite[3 * s + 1], b.gsite[3 * s + 2]};
+                rotate_s(q, gb, g);
                 dfr[3 * s + 0] = d0 + fmaf(iA[6], g[2], fmaf(iA[3], g[1], iA[0] * g[0]));
                 dfr[3 * s + 1] = d1 + fmaf(iA[7], g[2], fmaf(iA[4], g[1], iA[1] * g[0]));
                 dfr[3 * s + 2] = d2 + fmaf(iA[8], g[2], fmaf(iA[5], g[1], iA[2] * g[0]));
+                sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
             }
-        }
-        const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
-        float stc[NS], sts[NS], cr[NS], ci[NS];
-        const float kst = b.kstep[fw];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            sincospif(2.0f * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
-            cr[s] = 1.f; ci[s] = 0.f;
-        }
-        // the terms of one k-vector row (a few) are summed plainly, rows then compensated
-        float acc = 0.f, cacc = 0.f, row = 0.f;
-        for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
-            const int32_t kn = min(PA_KCHUNK32, k1 - kb);
-            for (int32_t x = lane; x < kn; x += 32) {
-                const int32_t kk = kb + x;
-                const float4 kc = b.kcoef4[kk];
-                s_kc[wp][x] = kc;
-                double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
-                ph -= rint(ph);
-                double sn, cs;
-                sincospi(2.0 * ph, &sn, &cs);
-                const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
-                // conj(S) e^{i phi} = (Sr cs + Si sn) + i (Sr sn - Si cs)
-                s_B[wp][x] = make_float2(float(Sr * cs + Si * sn), float(Sr * sn - Si * cs));
-            }
-            __syncwarp();
-            for (int32_t x = 0; x < kn; ++x) {
-                const float4 kc = s_kc[wp][x];
-                if (kc.w == 0.f) {  // row start: direct evaluation; the finished row enters the sum
-                    kahan_add(acc, cacc, row);
-                    row = 0.f;
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        // the phase reduced to [-1/2, 1/2] turns, then the hardware sine and
-                        // cosine (absolute error about 4e-7 on [-pi, pi])
-                        float ph = fmaf(kc.z, dfr[3 * s + 2], fmaf(kc.y, dfr[3 * s + 1], kc.x * dfr[3 * s]));
-                        ph -= rintf(ph);
-                        __sincosf(6.28318530717958648f * ph, &ci[s], &cr[s]);
-                    }
-                } else {  // next k-vector of the row
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        const float r = fmaf(cr[s], stc[s], -ci[s] * sts[s]);
-                        ci[s] = fmaf(cr[s], sts[s], ci[s] * stc[s]);
-                        cr[s] = r;
-                    }
-                }
-                float gr = 0.f, gi = 0.f;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) { gr = fmaf(gqs[s], cr[s], gr); gi = fmaf(gqs[s], ci[s], gi); }
-                const float2 B = s_B[wp][x];
-                row = fmaf(B.x, gr, fmaf(-B.y, gi, row));
-            }
-            __syncwarp();
-        }
-        kahan_add(acc, cacc, row);
-        if (active) w.dUr[li] = KE * (double(acc) - double(cacc));
-    }
-}
-
-// The reciprocal cross term in FP64 (the FP32 path's accurate form): the same tiles and row
-// recurrences as k_recip32, with the sites' fractional offsets from the bin centre, the phase
-// factors, the row starts (FP64 sincospi of the phase reduced to half a turn), the recurrences and
-// the sums all in FP64. Writes KE E_lr.
-template <int NS>
-__global__ void __launch_bounds__(32 * PA_WARPS32) k_recip64(DevBatch<float> b, CallArgs ca, Work w) {
-    __shared__ double2 s_B[PA_WARPS32][PA_KCHUNK32];
-    __shared__ float4 s_kc[PA_WARPS32][PA_KCHUNK32];
-    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    int32_t bin = 0, lo = 0, hi = 0;
-    while (next_tile(w, b.nbins, lane, bin, lo, hi)) {
-        const int32_t fw = b.bin_fw[bin];
-        const bool active = lo + lane < hi;
-        const int32_t li = active ? w.sorted[lo + lane] : 0;
-        float cx, cy, cz;
-        bin_centre(b, fw, bin, cx, cy, cz);
-        const float4 pa = active ? w.pose_a[li] : make_float4(cx, cy, cz, 0.f);
-        const float4 pq = active ? w.pose_b[li] : make_float4(0.f, 0.f, 0.f, 1.f);
-        const double* iA = b.invcells64 + 9 * fw;
-        const double d0 = double(pa.x) - double(cx), d1 = double(pa.y) - double(cy), d2 = double(pa.z) - double(cz);
-        double dfr[3 * NS];
-        {
+            float acc = 0.f, cacc = 0.f;
+            rows32<NS>(b.kcoef4, b.kS2, b.k_offsets[fw], b.k_offsets[fw + 1], dfr, stc, sts, gq32, cx, cy, cz, lane,
+                       s_B32[wp], s_kc[wp], acc, cacc);
+            E = double(acc) - double(cacc);
+        } else {
+            // FP64 site offsets from the bin centre
+            const double* iA = b.invcells64 + 9 * fw;
+            const double d0 = double(pa.x) - double(cx), d1 = double(pa.y) - double(cy), d2 = double(pa.z) - double(cz);
+            double dfr[3 * NS], stc[NS], sts[NS];
             const double q[4] = {double(pq.x), double(pq.y), double(pq.z), double(pq.w)};
+            const double kst = double(b.kstep[fw]);
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const double gb[3] = {b.gsite64[3 * s], b.gsite64[3 * s + 1], b.gsite64[3 * s + 2]};
@@ -427,57 +514,28 @@ __global__ void __launch_bounds__(32 * PA_WARPS32) k_recip64(DevBatch<float> b, 
                 dfr[3 * s + 0] = d0 + fma(iA[6], g[2], fma(iA[3], g[1], iA[0] * g[0]));
                 dfr[3 * s + 1] = d1 + fma(iA[7], g[2], fma(iA[4], g[1], iA[1] * g[0]));
                 dfr[3 * s + 2] = d2 + fma(iA[8], g[2], fma(iA[5], g[1], iA[2] * g[0]));
+                sincospi(2.0 * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
             }
-        }
-        const int32_t k0 = b.k_offsets[fw], k1 = b.k_offsets[fw + 1];
-        double stc[NS], sts[NS], cr[NS], ci[NS];
-        const double kst = double(b.kstep[fw]);
+            if (RMODE == 1) {
+                E = rows64<NS>(b.kcoef4, b.kS2, b.k_offsets[fw], b.k_offsets[fw + 1], dfr, stc, sts, gq64, cx, cy, cz,
+                               lane, s_B64[wp], s_kc[wp]);
+            } else {
+                E = rows64<NS>(b.ks64_coef, b.ks64_S2, b.ks64_off[fw], b.ks64_off[fw + 1], dfr, stc, sts, gq64, cx, cy,
+                               cz, lane, s_B64[wp], s_kc[wp]);
+                // the FP32 rows from the FP64 offsets rounded once
+                float dfr32[3 * NS], stc32[NS], sts32[NS];
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            sincospi(2.0 * kst * dfr[3 * s + 2], &sts[s], &stc[s]);
-            cr[s] = 1.0; ci[s] = 0.0;
-        }
-        double acc = 0.0;
-        for (int32_t kb = k0; kb < k1; kb += PA_KCHUNK32) {
-            const int32_t kn = min(PA_KCHUNK32, k1 - kb);
-            for (int32_t x = lane; x < kn; x += 32) {
-                const int32_t kk = kb + x;
-                const float4 kc = b.kcoef4[kk];
-                s_kc[wp][x] = kc;
-                double ph = double(kc.x) * double(cx) + double(kc.y) * double(cy) + double(kc.z) * double(cz);
-                ph -= rint(ph);
-                double sn, cs;
-                sincospi(2.0 * ph, &sn, &cs);
-                const double Sr = b.kS2[2 * kk], Si = b.kS2[2 * kk + 1];
-                s_B[wp][x] = make_double2(Sr * cs + Si * sn, Sr * sn - Si * cs);
-            }
-            __syncwarp();
-            for (int32_t x = 0; x < kn; ++x) {
-                const float4 kc = s_kc[wp][x];
-                if (kc.w == 0.f) {  // row start: direct evaluation
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        double ph = fma(double(kc.z), dfr[3 * s + 2], fma(double(kc.y), dfr[3 * s + 1],
-                                                                          double(kc.x) * dfr[3 * s]));
-                        ph -= rint(ph);
-                        sincospi(2.0 * ph, &ci[s], &cr[s]);
-                    }
-                } else {  // next k-vector of the row
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        const double r = fma(cr[s], stc[s], -ci[s] * sts[s]);
-                        ci[s] = fma(cr[s], sts[s], ci[s] * stc[s]);
-                        cr[s] = r;
-                    }
+                for (int s = 0; s < NS; ++s) {
+                    dfr32[3 * s] = float(dfr[3 * s]); dfr32[3 * s + 1] = float(dfr[3 * s + 1]);
+                    dfr32[3 * s + 2] = float(dfr[3 * s + 2]);
+                    stc32[s] = float(stc[s]); sts32[s] = float(sts[s]);
                 }
-                double gr = 0.0, gi = 0.0;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) { gr = fma(b.gq64[s], cr[s], gr); gi = fma(b.gq64[s], ci[s], gi); }
-                const double2 B = s_B[wp][x];
-                acc = fma(B.x, gr, fma(-B.y, gi, acc));
+                float acc = 0.f, cacc = 0.f;
+                rows32<NS>(b.ks32_coef, b.ks32_S2, b.ks32_off[fw], b.ks32_off[fw + 1], dfr32, stc32, sts32, gq32, cx,
+                           cy, cz, lane, s_B32[wp], s_kc[wp], acc, cacc);
+                E += double(acc) - double(cacc);
             }
-            __syncwarp();
         }
-        if (active) w.dUr[li] = KE * acc;
+        if (active) w.dUr[li] = KE * E;
     }
 }

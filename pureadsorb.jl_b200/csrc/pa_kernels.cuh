@@ -76,7 +76,16 @@ struct DevBatch {
     double gq64[PA_MAX_SITES_DEV];
     double rl2_64, re2_64;                        // the cutoffs squared, FP64
     F rn2;                                        // near radius squared (0: no near pairs)
-    int32_t recip64;                              // 1: the reciprocal term in FP64 (k_recip64)
+    int32_t rmode;                                // reciprocal term: 0 FP32, 1 FP64, 2 split tables (k_recip)
+    // the split tables of a charged FP32 batch: per framework the k-vectors of small |k| (FP64 rows)
+    // and the rest (FP32 rows), each in enumeration order with its own row-continuation flags
+    const float4* ks64_coef;
+    const double* ks64_S2;                        // 2*kpref*S (re, im)
+    const int32_t* ks64_off;                      // nfw+1
+    const float4* ks32_coef;
+    const double* ks32_S2;
+    const int32_t* ks32_off;                      // nfw+1
+    int32_t has_ksplit;
     F rl2_lo, rl2_hi, re2_lo, re2_hi;             // rounding bands around the cutoffs
 };
 
