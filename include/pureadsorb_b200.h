@@ -251,14 +251,21 @@ pa_status pa_rejection_tables(const pa_batch_desc* desc, const double* bs, const
 /* Allocation-free variant of pa_widom; no counterpart in the reference. For callers that may
  * not allocate device memory during the call (a host application that owns a fixed memory
  * budget, strict per-tenant accounting, or code that must avoid cudaMalloc's device-wide
- * synchronisation): the same kernels as pa_widom, with every per-call scratch buffer carved out
- * of one file-scope device array of 32 MiB that each GPU loading the library holds until the
- * process exits. Limits: at most 131,072 insertions per call (and, for an FP32 batch, 393,216
- * insertion-site pairs), 1,024 systems, 32,768 spatial bins and 65,536 rejection radii; larger
- * calls return PA_ERR_ARG. Only per_insertion->dU may be
- * requested. All calls share the array (host calls are serialised by a mutex); device work of two
- * calls must not overlap. The first call on a device looks up the array's address and should
- * come before any stream capture. */
+ * synchronisation): every per-call scratch buffer is carved out of one file-scope device array of
+ * 32 MiB that each GPU loading the library holds until the process exits. It computes what
+ * pa_widom computes (the same poses, phase-0 flags, energy and reduction kernels, and the context's
+ * FP32/FP64 split), except that on an FP32 batch the poses and phase 0 come from the fused
+ * per-insertion kernel (k_pose) instead of the warp-cooperative pair k_draw32 + k_phase0_32; both
+ * give the same poses and flags bit for bit. Limits: at most 131,072 insertions per call (and, for
+ * an FP32 batch, 393,216 insertion-site pairs), 1,024 systems, 32,768 spatial bins and 65,536
+ * rejection radii; larger calls return PA_ERR_ARG. Only per_insertion->dU may be requested.
+ * All calls share the array (host calls are serialised by a mutex); device work of two calls must
+ * not overlap. A call that returns an error after its device work began (a launch error, a
+ * timed-out wait) leaves the array in use until that work finishes; until then later calls return
+ * PA_ERR_STATE. The first call on a device looks up the array's address and creates an event,
+ * and the CUDA runtime may load the library's device module then (which allocates device memory,
+ * the array included): make one warm-up call before any stream capture and before the code that
+ * must not allocate. */
 pa_status pa_widom_static(pa_context* ctx, const pa_batch* batch, const pa_widom_args* args, pa_block_sums* sums,
                           pa_insertion_out* per_insertion);
 

@@ -1829,6 +1829,16 @@ namespace {
 
 std::mutex st_mutex;                 // serialises host calls: the scratch and staging are shared
 void* st_addr[64] = {nullptr};       // device address of pa_static_scratch, per device
+cudaEvent_t st_done[64] = {};        // recorded after each call's device work, per device
+bool st_busy[64] = {false};          // a call returned early: its device work may still use the array
+
+// Records the device's st_done event on the call's stream when the call returns, whatever path
+// it takes (so the next call can tell whether work an early return left behind has finished).
+struct StaticDone {
+    cudaEvent_t e;
+    cudaStream_t s;
+    ~StaticDone() { cudaEventRecord(e, s); }
+};
 unsigned char st_stage[ST_INPUT_END];  // host staging of the small per-call inputs
 int64_t st_ns[ST_MAX_SYS];
 Seg st_segs[ST_MAX_SEG];
@@ -1915,10 +1925,20 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
         cudaError_t e = cudaGetSymbolAddress(&p, pa_static_scratch);
         if (e != cudaSuccess || !p)
             return fail(ctx, PA_ERR_CUDA, std::string("cudaGetSymbolAddress(pa_static_scratch): ") + cudaGetErrorString(e));
+        if (cudaEventCreateWithFlags(&st_done[ctx->device], cudaEventDisableTiming) != cudaSuccess)
+            return fail(ctx, PA_ERR_CUDA, "pa_widom_static: event creation failed");
         st_addr[ctx->device] = p;
+    }
+    if (st_busy[ctx->device]) {
+        if (cudaEventQuery(st_done[ctx->device]) == cudaErrorNotReady)
+            return fail(ctx, PA_ERR_STATE, "pa_widom_static: the static scratch is still in use by the device work of "
+                                           "an earlier call that returned an error; retry once it has finished");
+        st_busy[ctx->device] = false;
     }
     char* base = static_cast<char*>(st_addr[ctx->device]);
     cudaStream_t st = ctx->stream;
+    st_busy[ctx->device] = true;  // cleared when this call's device work is known to be done
+    const StaticDone done{st_done[ctx->device], st};
     PA_CUDA(ctx, cudaMemcpyAsync(base, st_stage, ST_INPUT_END, cudaMemcpyHostToDevice, st));
     const int64_t nfine = int64_t(B->nbins) * nsub;
     PA_CUDA(ctx, cudaMemsetAsync(base + ST_BIN_COUNT, 0, sizeof(int32_t) * (nfine + 1), st));
@@ -1977,6 +1997,7 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
         PA_CUDA(ctx, cudaMemcpyAsync(per->dU + i_lo, base + ST_DU, sizeof(double) * n_act, cudaMemcpyDeviceToHost, st));
     pa_status ws = wait_stream(ctx);
     if (ws != PA_OK) return ws;
+    st_busy[ctx->device] = false;
     if (st_counters[2] != 0 || st_counters[10] != 0)
         return fail(ctx, PA_ERR_TIMEOUT, "a bounded wait on a bulk copy gave up inside the energy kernel");
     if (sums->segments)
