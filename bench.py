@@ -29,7 +29,9 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM 
 # DRAM bytes (read + write) of one k_energy32 launch on this workload, per bin width (the
 # autotuner's choice), from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum); they
 # cannot be measured inside the bench
-ENERGY32_TRAFFIC_BYTES = {3.0: 83.832064e6 + 8.302592e6, 3.5: 70.104320e6 + 7.413248e6}
+# (with the default FP32/FP64 split)
+ENERGY32_TRAFFIC_BYTES = {3.0: 129.783040e6 + 10.789632e6}
+FP64_PEAK_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12  # TFLOP/s: 64 FP64 FMA lanes per SM
 # the metric and workload names of both arms (ours and the reference's CPU implementation)
 METRIC = "Widom insertions/s (CO2, 5,832-atom framework)"
 WORKLOAD = "co2_5832_atoms_3x3x3_monoclinic"
@@ -48,6 +50,9 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-fit", action="store_true")
     p.add_argument("--no-chain", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the per-insertion parity fractions")
+    p.add_argument("--no-ch4", action="store_true", help="skip the CH4 configuration")
+    p.add_argument("--no-all-fp32", action="store_true", help="skip the all-FP32 comparison steps")
     p.add_argument("--no-tune", action="store_true", help="default bin width and grid (e.g. for profiling)")
     p.add_argument("--bin-width", type=float, default=0.0, help="with --no-tune: this bin width (Å) instead of 3.0")
     return p.parse_args()
@@ -128,16 +133,17 @@ def workload(pa, T):
     return pa.FrameworkBatch(fws, ff, guest, ewald), guest, prm
 
 
-def count_pairs(batch, poses):
-    """Mean numbers of (site, atom) pairs inside the LJ and the Ewald cutoff per insertion, for
-    survivors' poses (fractional position, quaternion) of a one-framework batch: one minimum
-    image per atom, as the reference's insertion_energy visits them (numpy, FP64)."""
+def count_pairs(batch, poses, near_radius=0.0):
+    """Mean numbers of (site, atom) pairs inside the LJ and the Ewald cutoff per insertion, and
+    of pairs inside either cutoff closer than near_radius, for survivors' poses (fractional
+    position, quaternion) of a one-framework batch: one minimum image per atom, as the
+    reference's insertion_energy visits them (numpy, FP64)."""
     A = np.asarray(batch.cells[0])
     iA = np.linalg.inv(A)
     atoms = np.asarray(batch.positions)
     sites = np.asarray(batch.guest_sites_orig)
     rl2, re2 = batch.cutoff ** 2, batch.ewald_cutoff ** 2
-    nl = ne = 0
+    nl = ne = nn = 0
     for p in poses:
         pos = A @ p[:3]
         u, w = p[3:6], p[6]
@@ -149,8 +155,9 @@ def count_pairs(batch, poses):
             r2 = np.einsum("ij,ij->i", d, d)
             nl += int(np.sum(r2 < rl2))
             ne += int(np.sum(r2 < re2))
+            nn += int(np.sum((r2 < near_radius ** 2) & ((r2 < rl2) | (r2 < re2))))
     n = max(1, len(poses))
-    return nl / n, ne / n
+    return nl / n, ne / n, nn / n
 
 
 class OracleWorkload:
@@ -359,6 +366,71 @@ def batched_workload(pa, backend, torch, stream, flush):
                                    "is tests/test_gpu_batched.py"}}
 
 
+def ch4_workload(pa, backend, torch, stream, flush):
+    """The plain FP64 LJ-only CH4 configuration (cubic P1, a = 25.832 A, 424 atoms of 4 types,
+    united-atom CH4, 12.8 A cutoff, 10^5 insertions, seed 42, T = 298.15 K, 10 blocks), in both
+    forms: mu_ex, K_H, q_st with their block standard errors, and insertions/s from CUDA events
+    around one widom call (median of 5, batch resident)."""
+    fws, ff, guest, ewald, prm = pa.synthetic.lj_ch4()
+    out = {"workload": "lj_ch4_424_atoms_cubic", "ninsert": prm["ninsert"], "seed": prm["seed"], "T_K": prm["T"],
+           "nblocks": prm["nblocks"]}
+    for name, T in (("fp64_plain", np.float64), ("fp32", np.float32)):
+        b = pa.FrameworkBatch(fws, ff, guest, ewald, T=T)
+        call = lambda: pa.widom(b, guest, T=prm["T"], ninsert=prm["ninsert"], seed=prm["seed"], nblocks=prm["nblocks"],
+                                backend=backend)
+        for _ in range(3):
+            r = call()[0]
+        ms = []
+        for _ in range(5):
+            flush.zero_()
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = call()[0]
+            e.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(e))
+        out[name] = {"mu_ex_eV": r.mu_ex, "mu_ex_err": r.mu_ex_err, "K_H": r.K_H, "K_H_err": r.K_H_err,
+                     "q_st_eV": r.q_st, "q_st_err": r.q_st_err, "nsamples": r.nsamples,
+                     "ms_per_call": float(np.median(ms)), "value": prm["ninsert"] / (float(np.median(ms)) / 1e3),
+                     "unit": "insertions/s"}
+        b.drop_device()
+    out["dlnKH_fp32_vs_fp64"] = abs(math.log(out["fp32"]["K_H"]) - math.log(out["fp64_plain"]["K_H"]))
+    out["dqst_eV_fp32_vs_fp64"] = abs(out["fp32"]["q_st_eV"] - out["fp64_plain"]["q_st_eV"])
+    return out
+
+
+def parity_fractions(pa, orc, backend, n=20_000):
+    """Per workload, the fraction of survivors whose FP32 dU lies within max(1e-5 |dU|, 8.62e-8 eV)
+    of the FP64 oracle at the same poses, with the default split and with every pair and the
+    reciprocal term in FP32; and the worst error in units of that tolerance."""
+    ctx = backend.ctx
+    default = ctx.fp32_split()
+    out = {}
+    for name, gen, seed in (("co2_5832_atoms", pa.synthetic.co2, 42), ("lj_ch4_424_atoms", pa.synthetic.lj_ch4, 42)):
+        fws, ff, guest, ewald = gen(T=np.float32)[:4]
+        b = pa.FrameworkBatch(fws, ff, guest, ewald)
+        kT = float(np.float32(pa.KB * 298.15))
+        v, keep = orc.view(b, b.guest_sites_orig, b.guest_charges_orig, b.cutoff, b.ewald_cutoff)
+        rho2, reach0 = pa.build_rejection_tables(b, kT)
+        ref = orc.widom(v, 32, kT, n, seed, 10, pa.default_run(n, 1), True, rho2, reach0)
+        surv = ref["flags"] == 0
+        res = {"insertions": n, "survivors": int(surv.sum())}
+        for mode, rn, r64 in (("default", default.near_radius, default.fp64_reciprocal), ("all_fp32", 0.0, 0)):
+            ctx.set_fp32_split(near_radius=rn, fp64_reciprocal=r64)
+            ins = {}
+            pa._widom(b, guest, reject=True, T=298.15, ninsert=n, seed=seed, nblocks=10, backend=backend,
+                      insertions=ins)
+            a, r = ins["dU"][surv], ref["dU"][surv]
+            tol = np.maximum(1e-5 * np.abs(r), 8.62e-8)
+            res[mode] = {"near_radius": rn, "fp64_reciprocal": bool(r64),
+                         "fraction_within": float(np.mean(np.abs(a - r) <= tol)),
+                         "worst_over_tolerance": float(np.max(np.abs(a - r) / tol))}
+        ctx.set_fp32_split(near_radius=default.near_radius, fp64_reciprocal=default.fp64_reciprocal)
+        b.drop_device()
+        out[name] = res
+    return out
+
+
 def fitting_workload(pa, backend):
     """Adam on the 8 palette scale factors of 128 frameworks, 2^18 insertions per framework per
     step (batched FP32 widom + adjoint), targets from the plain FP64 form at the hidden factors."""
@@ -514,7 +586,8 @@ def main():
         pa._widom(batch, guest, reject=True, T=prm["T"], ninsert=sample_n, seed=prm["seed"], nblocks=nblocks,
                   backend=backend, insertions=ins)
         surv_frac = float(np.mean(ins["flags"] == 0))
-        n_lj, n_ew = count_pairs(batch, ins["poses"][ins["flags"] == 0][:512])
+        rn = ctx.fp32_split().near_radius
+        n_lj, n_ew, n_near = count_pairs(batch, ins["poses"][ins["flags"] == 0][:512], rn)
         dev = batch.device(ctx)
         list_entries, nbins = dev.info()
         L = list_entries / nbins
@@ -522,26 +595,34 @@ def main():
         nk = int(batch.k_offsets[1])
         kc = batch.kcoeffs
         rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
-        # executed FP32 work of k_energy32 per survivor (FMA = 2 flops):
-        # each of its N (insertion, site) items walks its bin's list, 8 flops per entry for the
-        # distance, and 52 per in-cutoff pair (LJ 10 + screened Coulomb 38 + compensated add 4).
-        # The reciprocal term (k_recip32: 10 per (k, site) + 7 per k for the recurrence, 25 per
-        # (row start, site)) runs in its own kernel and is reported beside it.
-        flops_surv = 8 * N * L + 52 * n_lj
+        # executed work of k_energy32 per survivor (FMA = 2 flops): each of its N (insertion,
+        # site) items walks its bin's list, 8 FP32 flops per entry for the distance; a pair in
+        # the cutoff takes 52 FP32 flops (LJ 10 + screened Coulomb 38 + compensated add 4), or,
+        # closer than the near radius, 54 FP64 flops (distance 8, LJ 7, screened Coulomb 38,
+        # sum 1). The bound is the FP32 flops at the FP32 FMA peak plus the FP64 flops at the
+        # FP64 peak; `achieved` is the FP32-equivalent rate (FP64 flops weighted by the peak
+        # ratio), so frac = that bound's time / the measured time. The reciprocal term
+        # (10 per (k, site) + 7 per k, 25 per (row start, site)) runs in its own kernel.
+        flops32 = 8 * N * L + 52 * (n_lj - n_near)
+        flops64 = 54 * n_near
+        peak = fp32_peak(torch)
+        flops_surv = flops32 + flops64 * (peak / FP64_PEAK_NOMINAL)
         flops_recip = (10 * N + 7) * nk + 25 * N * rows
         e_ms = kms[2] / max(1, kn[2])
         surv_per_launch = surv_frac * (s1 - s0) * (ninsert / nseg)
         achieved = flops_surv * surv_per_launch / (e_ms / 1e3) / 1e12
-        peak = fp32_peak(torch)
         ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
-        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+        roof = {"bound": "fp32+fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": ENERGY32_TRAFFIC_BYTES.get(float(tune.bin_width))
-                if (args.ninsert == 1_000_000 and world == 1) else None,
+                if (args.ninsert == 1_000_000 and world == 1 and rn == 6.0) else None,
                 "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
-                "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz)",
-                "flops_per_survivor": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
+                "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz); "
+                             "FP64 flops weighted by FP32/FP64 nominal peaks (74.4 / 37.2 TFLOP/s)",
+                "fp32_flops_per_survivor": flops32, "fp64_flops_per_survivor": flops64,
+                "flops_per_survivor_fp32_equivalent": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
                 "reciprocal_combine_ms_per_step": kms[6] / args.steps, "reference_algorithm_flops_per_survivor": ref_alg,
-                "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew}
+                "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew,
+                "pairs_fp64": n_near}
 
         # plain FP64 form on the same workload and stream (the >= 3x denominator)
         fp64 = None
@@ -561,7 +642,10 @@ def main():
             r32 = pa.widom(batch, guest, T=prm["T"], ninsert=n64, seed=prm["seed"], nblocks=nblocks, backend=backend)
             fp64 = {"value": rate64, "unit": "insertions/s", "ninsert": n64, "ratio_fp32_over_fp64": value / world / rate64,
                     "dlnKH": abs(math.log(r32[0].K_H) - math.log(r64[0].K_H)),
-                    "dqst_eV": abs(r32[0].q_st - r64[0].q_st)}
+                    "dqst_eV": abs(r32[0].q_st - r64[0].q_st),
+                    "note": "k_energy64 as it is: the plain FP64 reference algorithm, one thread per survivor over "
+                            "every atom (min image per atom), with about 7 of 32 lanes active (divergent cutoff "
+                            "branches); the ratio is against that kernel"}
 
         # end to end through the public API from host arrays (batch re-uploaded each step)
         e2e_ms = []
@@ -610,6 +694,31 @@ def main():
                    "parameters": int(2 * len(ff.names) + len(gr[0].charges)),
                    "note": "widom_grad: forward pass + adjoint pass + host chain rule, CUDA events around the call"}
 
+        # the same steps with every pair and the reciprocal term in FP32 (the cost of the default
+        # split's FP64 near pairs and reciprocal term)
+        fast = None
+        if world == 1 and not args.no_all_fp32:
+            split = ctx.fp32_split()
+            ctx.set_fp32_split(near_radius=0.0, fp64_reciprocal=False)
+            step()
+            step()
+            torch.cuda.synchronize()
+            fms = []
+            for i in range(args.steps):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                step()
+                b.record(stream)
+                torch.cuda.synchronize()
+                fms.append(a.elapsed_time(b))
+            ctx.set_fp32_split(near_radius=split.near_radius, fp64_reciprocal=split.fp64_reciprocal)
+            fast = {"near_radius": 0.0, "fp64_reciprocal": False, "ms_per_step": float(np.mean(fms)),
+                    "value": ninsert / (float(np.mean(fms)) / 1e3), "unit": "insertions/s",
+                    "note": "every pair and the reciprocal term in FP32: meets the aggregate bounds, not the "
+                            "per-insertion one (see parity)"}
+        parity = None if world > 1 or args.no_parity else parity_fractions(pa, orc, backend)
+        ch4 = None if world > 1 or args.no_ch4 else ch4_workload(pa, backend, torch, stream, flush)
         batched = None if args.no_batched or world > 1 else batched_workload(pa, backend, torch, stream, flush)
         chain = None if args.no_chain or world > 1 else chain_workload(pa, orc, backend, torch, stream, flush,
                                                                        no_cpu=args.no_cpu)
@@ -628,7 +737,15 @@ def main():
                 "dtype": "f32", "data": "synthetic",
                 "config": bench_config(args.ninsert, world, int(len(batch.positions)), nk, prm),
                 "result": {"mu_ex": res32.mu_ex, "mu_ex_err": res32.mu_ex_err, "K_H": res32.K_H,
-                           "K_H_err": res32.K_H_err, "q_st": res32.q_st, "q_st_err": res32.q_st_err},
+                           "K_H_err": res32.K_H_err, "q_st": res32.q_st, "q_st_err": res32.q_st_err,
+                           "note": "this synthetic framework is so dense that a handful of insertions carry "
+                                   "nearly all the weight (K_H_err / K_H large); the batched and CH4 sections "
+                                   "are the meaningful aggregate comparisons"},
+                "fp32_split": {"near_radius": ctx.fp32_split().near_radius,
+                               "fp64_reciprocal": bool(ctx.fp32_split().fp64_reciprocal)},
+                "all_fp32": fast,
+                "parity": parity,
+                "ch4_config": ch4,
                 "clocks": clk.summary(),
                 "tuning": {"bin_width": tune.bin_width, "ctas_per_sm": tune.ctas_per_sm, "cuda_graphs": True,
                            "candidates": [list(r) for r in tune.table]},
