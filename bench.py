@@ -448,6 +448,20 @@ def fitting_workload(pa, backend):
     build_s = time.perf_counter() - t0
     res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
                                lr=prm["lr"], seed=seed, backend=backend)
+    # what the data determine: the loss's Gauss-Newton curvature at the start and at the end, the
+    # parameter error along its eigenvectors, and each type's eps sigma^6 against the hidden one
+    ones = np.ones(len(prm["hidden"]))
+    ident = {}
+    for name, xv in (("initial", ones), ("final", res.x)):
+        idf = pa.fit.identifiability(b, guest, ff, prm["fitted_types"], xv, targets, T=T, ninsert=n, seed=seed,
+                                     backend=backend, x_ref=prm["hidden"])
+        ident[name] = {"hessian_eigenvalues": idf.eigenvalues.tolist(), "error_along_eigenvectors":
+                       idf.error_along.tolist(), "loss_along_eigenvectors": idf.loss_along.tolist(),
+                       "eps_sigma6_rel_error": idf.eps_sigma6_rel_error.tolist()}
+    lam = np.asarray(ident["final"]["hessian_eigenvalues"])
+    stiff = lam >= 1e-2 * lam[0]
+    err_f = np.asarray(ident["final"]["error_along_eigenvectors"])
+    err_i = np.asarray(ident["initial"]["error_along_eigenvectors"])
     return {"workload": "fitting_128_frameworks_palette4", "frameworks": len(fws), "natoms": int(len(b.positions)),
             "ninsert_per_step": n, "steps": prm["steps"], "lr": prm["lr"],
             "frameworks_fitted": int(np.sum(np.isfinite(targets))),
@@ -456,6 +470,15 @@ def fitting_workload(pa, backend):
             "max_scale_error_initial": float(np.max(np.abs(1 - prm["hidden"]))),
             "max_scale_error_final": float(np.max(np.abs(res.x - prm["hidden"]))),
             "scales_final": res.x.tolist(), "scales_hidden": prm["hidden"].tolist(),
+            "identifiability": ident,
+            "stiff_directions": int(stiff.sum()),
+            "error_in_stiff_directions_initial": float(np.linalg.norm(err_i[stiff])),
+            "error_in_stiff_directions_final": float(np.linalg.norm(err_f[stiff])),
+            "error_in_soft_directions_final": float(np.linalg.norm(err_f[~stiff])),
+            "max_eps_sigma6_rel_error_initial": float(np.max(ident["initial"]["eps_sigma6_rel_error"])),
+            "max_eps_sigma6_rel_error_final": float(np.max(ident["final"]["eps_sigma6_rel_error"])),
+            "identifiability_note": "stiff directions: Gauss-Newton eigenvalues >= 1e-2 of the largest at the fitted "
+                                    "point; the error norms are of (x - hidden) projected on the eigenvectors",
             "targets_s": target_s, "batch_build_s": build_s}
 
 

@@ -91,3 +91,45 @@ def fit_lj_scales(batch, guest, ff, types, targets, *, T, ninsert, steps=200, lr
         out.xs.append(x.copy())
     out.x = x
     return out
+
+
+@dataclass
+class Identifiability:
+    """The loss's curvature at a point of the fit, from the adjoint Jacobian J (systems x scale
+    factors) of ln K_H: the Gauss-Newton Hessian H = (2/n) J^T J, its eigenvalues (descending) and
+    eigenvectors (columns), and, given reference scale factors, the parameter error split along
+    those eigenvectors and the relative error of each type's eps sigma^6 (the dispersion
+    coefficient, the combination ln K_H depends on most directly)."""
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray
+    error_along: np.ndarray = None       # |v_i . (x - x_ref)| per eigenvector
+    loss_along: np.ndarray = None        # lambda_i (v_i . (x - x_ref))^2: its share of the loss
+    eps_sigma6_rel_error: np.ndarray = None
+
+
+def identifiability(batch, guest, ff, types, x, targets, *, T, ninsert, seed=0, nblocks=10, backend=None,
+                    x_ref=None):
+    """Identifiability at scale factors x (one widom_grad call): see Identifiability."""
+    k = len(types)
+    idx = np.array([ff.typeindex(t) - 1 for t in types])
+    sig0, eps0 = type_parameters(ff)
+    ffx = scaled_forcefield(ff, types, x)
+    b = batch.with_forcefield(ffx, move_device=True, device_bounds=True)
+    lnk, grads = widom_grad(b, guest, ffx, T=T, ninsert=ninsert, backend=backend, seed=seed, nblocks=nblocks,
+                            reduce=False, charges=False)
+    use = np.isfinite(lnk) & np.isfinite(np.asarray(targets, dtype=np.float64))
+    J = np.array([np.concatenate([g.epsilon[idx] * eps0[idx], g.sigma[idx] * sig0[idx]])
+                  for g, u in zip(grads, use) if u])
+    H = 2.0 * J.T @ J / len(J)
+    lam, V = np.linalg.eigh(H)
+    order = np.argsort(-lam)
+    out = Identifiability(lam[order], V[:, order])
+    if x_ref is not None:
+        d = np.asarray(x, dtype=np.float64) - np.asarray(x_ref, dtype=np.float64)
+        proj = out.eigenvectors.T @ d
+        out.error_along = np.abs(proj)
+        out.loss_along = out.eigenvalues * proj**2
+        xr = np.asarray(x_ref, dtype=np.float64)
+        xx = np.asarray(x, dtype=np.float64)
+        out.eps_sigma6_rel_error = np.abs(xx[:k] * xx[k:] ** 6 / (xr[:k] * xr[k:] ** 6) - 1.0)
+    return out

@@ -65,3 +65,18 @@ def test_adam_recovers_hidden_scales(pa, palette):
     assert res.loss[-1] < 1e-3 * res.loss[0]
     assert err < err0
     assert np.linalg.norm(res.x - prm["hidden"]) < np.linalg.norm(1.0 - prm["hidden"])
+    # what the data determine: along the loss's stiffest curvature directions (Gauss-Newton
+    # eigenvectors at the fitted point) the error falls far more than the raw parameter error
+    kw = dict(T=T_K, ninsert=n, seed=prm["seed"], backend=be, x_ref=prm["hidden"])
+    fin = pa.fit.identifiability(b, guest, ff, prm["fitted_types"], res.x, targets, **kw)
+    ini = pa.fit.identifiability(b, guest, ff, prm["fitted_types"], np.ones(8), targets, **kw)
+    V = fin.eigenvectors
+    stiff = fin.eigenvalues >= 1e-2 * fin.eigenvalues[0]
+    e0 = np.abs(V.T @ (1.0 - prm["hidden"]))
+    e1 = fin.error_along
+    print(f"curvature eigenvalues {np.array2string(fin.eigenvalues, precision=2)}; error along them "
+          f"{np.array2string(e0, precision=3)} -> {np.array2string(e1, precision=3)}; eps sigma^6 rel error "
+          f"{np.array2string(ini.eps_sigma6_rel_error, precision=3)} -> "
+          f"{np.array2string(fin.eps_sigma6_rel_error, precision=3)}")
+    assert stiff.sum() >= 1
+    assert np.linalg.norm(e1[stiff]) < 0.2 * np.linalg.norm(e0[stiff])
