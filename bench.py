@@ -307,8 +307,11 @@ def batched_workload(pa, backend, torch, stream, flush):
     ctx = backend.ctx
     fws, ff, guest, ewald, prm = pa.synthetic.batched(T=np.float32)
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws, ff, guest, ewald, sk=ctx.structure_factor, self_term=ctx.self_term)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, device=ctx)
     build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pa.FrameworkBatch(fws, ff, guest, ewald, sk=ctx.structure_factor, self_term=ctx.self_term)
+    build_host_tables_s = time.perf_counter() - t0
     n, T, seed, nb = prm["ninsert"], prm["T"], prm["seed"], prm["nblocks"]
     tune = pa.autotune(b, guest, T=T, ninsert=n, backend=backend, seed=seed, nblocks=nb, bin_widths=(3.0, 3.5, 4.0),
                        ctas_per_sm=(8,), repeats=1)
@@ -354,7 +357,10 @@ def batched_workload(pa, backend, torch, stream, flush):
     b64.drop_device()
     return {"workload": "batched_64_frameworks", "frameworks": len(fws), "natoms": int(len(b.positions)),
             "coupled_k": int(b.k_offsets[-1]), "ninsert": n, "ms_per_call": ms_call, "value": n / (ms_call / 1e3),
-            "unit": "insertions/s", "batch_build_s": build_s, "tuning": {"bin_width": tune.bin_width,
+            "unit": "insertions/s", "batch_build_s": build_s,
+            "batch_build_note": "every table the device can build built there (FrameworkBatch(device=ctx)); "
+                                "batch_build_host_tables_s: k-vectors, kmin and cell sort on the host instead",
+            "batch_build_host_tables_s": build_host_tables_s, "tuning": {"bin_width": tune.bin_width,
                                                                          "ctas_per_sm": tune.ctas_per_sm,
                                                                          "cuda_graphs": True},
             "fp64_plain": {"value": rate64, "ninsert": n64, "ratio_fp32_over_fp64": n / (ms_call / 1e3) / rate64,
@@ -443,11 +449,16 @@ def fitting_workload(pa, backend):
                                  sk=ctx.structure_factor, self_term=ctx.self_term)
     target_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, sk=ctx.structure_factor, self_term=ctx.self_term,
-                          bounds=ctx.batch_bounds)
+    b = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32, device=ctx, bounds=ctx.batch_bounds)
     build_s = time.perf_counter() - t0
-    res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
-                               lr=prm["lr"], seed=seed, backend=backend)
+    # each step's rejection radii from the device as well
+    tables = backend.device_tables
+    backend.device_tables = True
+    try:
+        res = pa.fit.fit_lj_scales(b, guest, ff, prm["fitted_types"], targets, T=T, ninsert=n, steps=prm["steps"],
+                                   lr=prm["lr"], seed=seed, backend=backend)
+    finally:
+        backend.device_tables = tables
     # what the data determine: the loss's Gauss-Newton curvature at the start and at the end, the
     # parameter error along its eigenvectors, and each type's eps sigma^6 against the hidden one
     ones = np.ones(len(prm["hidden"]))

@@ -248,6 +248,40 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* batch, const pa_widom_args* 
 pa_status pa_rejection_tables(const pa_batch_desc* desc, const double* bs, const double* kmin, double kT, double eps_F,
                               double* rho2, int32_t* reach0, int32_t* bad_system);
 
+/* Batch construction on the device (pose-independent tables; the host builder computes the same
+ * ones). Each call copies its host inputs, runs on the context's stream and returns once its
+ * outputs are in host memory.
+ *
+ * pa_batch_rejection_tables: pa_rejection_tables for an uploaded batch, the root searches
+ * (find_rho2, src/reject.jl:168-209) on the device, one thread per (system, site, type), with the
+ * same operation sequence as the host, so rho2 and reach0 equal pa_rejection_tables' bit for bit.
+ * bs (nfw) and kmin (nfw*N*nt) as for pa_rejection_tables; the pair tables and constant offsets
+ * are the batch's (after any pa_batch_set_pair_tables). */
+pa_status pa_batch_rejection_tables(pa_context* ctx, const pa_batch* batch, const double* bs, const double* kmin,
+                                    double kT, double eps_F, double* rho2, int32_t* reach0, int32_t* bad_system);
+
+/* The half-space k-vectors of one cell (`kvectors`, src/ewald.jl:142-157): n1 = 0..nmax[0],
+ * n2 = -nmax[1]..nmax[1], n3 = -nmax[2]..nmax[2] (n3 fastest), (0,0,0) left out, |k| <= kmax,
+ * with k = B (n1, n2, n3) for the reciprocal basis B (row-major 3x3, 2 pi (A^-1)^T), weight 1 for
+ * n1 = 0 and 2 otherwise, and kpref = w (c2piv exp(-|k|^2 / four_a2) / |k|^2) (`pk`,
+ * src/ewald.jl:36-39) with c2piv = 2 pi / V and four_a2 = 4 alpha^2. Outputs in enumeration order:
+ * ks (3 per k-vector), weights, kpref, coeffs (3 per k-vector), and their number in *nk; the
+ * arrays need room for (nmax[0]+1)(2nmax[1]+1)(2nmax[2]+1)-1 k-vectors (capacity). */
+pa_status pa_kvectors(pa_context* ctx, const double* B, const int32_t* nmax, double kmax, double c2piv, double four_a2,
+                      int64_t capacity, double* ks, double* weights, double* kpref, int32_t* coeffs, int64_t* nk);
+
+/* kmin of one framework (`kmin_table`, src/reject.jl:134-145): kmin[a*ntypes + t] is the most
+ * negative KE q_a q_h over its atoms h of compact type t+1 (types 1-based), or 0. */
+pa_status pa_kmin_table(pa_context* ctx, const double* guest_charges, int32_t nguest, const int32_t* types,
+                        const double* charges, int64_t natoms, int32_t ntypes, double* kmin);
+
+/* The phase-0 cell list of one framework (`cell_sort`, src/cell.jl:96-118): the stable counting
+ * sort of its atoms by the cell of their wrapped fractional coordinates (3 per atom) on an
+ * ncells[0] x ncells[1] x ncells[2] grid (x fastest). perm[i] is the 0-based original index of the
+ * i-th sorted atom; offsets (prod(ncells)+1) the start of every cell. */
+pa_status pa_cell_sort(pa_context* ctx, const double* frac, int64_t natoms, const int32_t* ncells, int64_t* perm,
+                       int32_t* offsets);
+
 /* Allocation-free variant of pa_widom; no counterpart in the reference. For callers that may
  * not allocate device memory during the call (a host application that owns a fixed memory
  * budget, strict per-tenant accounting, or code that must avoid cudaMalloc's device-wide

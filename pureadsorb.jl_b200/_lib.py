@@ -2,6 +2,7 @@
 in-tree by build.py). Every call checks its status and raises with the library's message; a
 missing library raises LibraryMissing: there is no fallback path."""
 import atexit
+import math
 import ctypes
 import os
 import weakref
@@ -83,6 +84,10 @@ SIGNATURES = [
     ("pa_context_kernel_times", _i32, [_p, _p, _p]),
     ("pa_context_set_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
     ("pa_context_get_tuning", _i32, [_p, ctypes.POINTER(Tuning)]),
+    ("pa_batch_rejection_tables", _i32, [_p, _p, _p, _p, _f64, _f64, _p, _p, _p]),
+    ("pa_kvectors", _i32, [_p, _p, _p, _f64, _f64, _f64, _i64, _p, _p, _p, _p, _p]),
+    ("pa_kmin_table", _i32, [_p, _p, _i32, _p, _p, _i64, _i32, _p]),
+    ("pa_cell_sort", _i32, [_p, _p, _i64, _p, _p, _p]),
     ("pa_context_set_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
     ("pa_context_get_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
     ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
@@ -257,6 +262,43 @@ class Context:
         return S[0::2] + 1j * S[1::2]
 
 
+    def kvectors(self, B, nmax, kmax, alpha, V):
+        """The half-space k-vectors of one cell on the device (pa_kvectors): (ks (nk, 3), weights,
+        kpref, coefficients (nk, 3)) in enumeration order, from the reciprocal basis B (3 x 3), the
+        bounds nmax (3) and the cell's volume V; kpref = w 2 pi / V exp(-k^2 / 4 alpha^2) / k^2."""
+        Bc = np.ascontiguousarray(B, dtype=np.float64).reshape(9)
+        nm = np.ascontiguousarray(nmax, dtype=np.int32).reshape(3)
+        cap = max(1, int((nm[0] + 1) * (2 * nm[1] + 1) * (2 * nm[2] + 1)) - 1)
+        ks, w, kp = np.zeros(3 * cap), np.zeros(cap), np.zeros(cap)
+        co = np.zeros(3 * cap, dtype=np.int32)
+        nk = _i64()
+        self.check(lib().pa_kvectors(self.handle, ptr(Bc), ptr(nm), float(kmax), 2 * math.pi / float(V),
+                                     4 * float(alpha) ** 2, cap, ptr(ks), ptr(w), ptr(kp), ptr(co), ctypes.byref(nk)),
+                   "pa_kvectors")
+        n = nk.value
+        return ks[:3 * n].reshape(n, 3), w[:n], kp[:n], co[:3 * n].reshape(n, 3)
+
+    def kmin_table(self, guest_charges, types, charges, ntypes):
+        """kmin (N x ntypes) of one framework's atoms (types 1-based) on the device (pa_kmin_table)."""
+        g = np.ascontiguousarray(guest_charges, dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        out = np.zeros(len(g) * int(ntypes))
+        self.check(lib().pa_kmin_table(self.handle, ptr(g), len(g), ptr(t), ptr(q), len(q), int(ntypes), ptr(out)),
+                   "pa_kmin_table")
+        return out.reshape(len(g), int(ntypes))
+
+    def cell_sort(self, frac, n):
+        """(permutation, prod(n)+1 offsets) of the stable cell sort of one framework's atoms on the
+        device (pa_cell_sort)."""
+        f = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, 3)
+        nn = np.ascontiguousarray(n, dtype=np.int32).reshape(3)
+        perm = np.zeros(len(f), dtype=np.int64)
+        off = np.zeros(int(nn[0]) * int(nn[1]) * int(nn[2]) + 1, dtype=np.int32)
+        self.check(lib().pa_cell_sort(self.handle, ptr(f), len(f), ptr(nn), ptr(perm), ptr(off)), "pa_cell_sort")
+        return perm, off
+
+
 class DeviceBatch:
     """A batch uploaded to a context for one precision (pa_batch)."""
 
@@ -283,6 +325,20 @@ class DeviceBatch:
         bs = np.zeros(nfw)
         self.ctx.check(lib().pa_batch_hardcore_bounds(self.ctx.handle, self.handle, ptr(bs)), "pa_batch_hardcore_bounds")
         return bs
+
+    def rejection_tables(self, bs, kmin, kT, eps_F, nsys, N, nt):
+        """Rejection radii (nsys*N*nt) and stencil reaches (nsys x 3) of one call, the root searches
+        on the device (pa_batch_rejection_tables); returns (rho2, reach0, bad system or 0)."""
+        b = np.ascontiguousarray(bs, dtype=np.float64)
+        k = np.ascontiguousarray(kmin, dtype=np.float64)
+        rho2 = np.zeros(nsys * N * nt)
+        reach0 = np.zeros((nsys, 3), dtype=np.int32)
+        bad = _i32(0)
+        st = lib().pa_batch_rejection_tables(self.ctx.handle, self.handle, ptr(b), ptr(k), float(kT), float(eps_F),
+                                             ptr(rho2), ptr(reach0), ctypes.byref(bad))
+        if st != PA_OK and bad.value == 0:
+            self.ctx.check(st, "pa_batch_rejection_tables")
+        return rho2, reach0, bad.value
 
     def info(self):
         a, b = _i64(), _i64()

@@ -76,10 +76,21 @@ class FrameworkBatch:
     computes the hard-core bounds B_s from the finished batch (batch -> array of one per
     framework); `bounds=Context.batch_bounds` evaluates them on the device (FP64, equal to the
     host's to rounding) through the batch's upload to that context, which later calls reuse.
+    `kv`, `kmin` and `cellsort` take the k-vector enumeration with its prefactors, the kmin table and
+    the phase-0 cell sort (signatures of `Context.kvectors`, `Context.kmin_table` and
+    `Context.cell_sort`); `device=Context` sets sk, self_term, kv, kmin and cellsort to that
+    context's device versions at once (the tables equal the host's bit for bit, the structure
+    factors, self terms and prefactors to rounding).
     """
 
     def __init__(self, fws, ff, guest, ewald, cellwidth=2, fullk=False, T=None, sk=None, self_term=None,
-                 bounds=None):
+                 bounds=None, kv=None, kmin=None, cellsort=None, device=None):
+        if device is not None:
+            sk = sk or device.structure_factor
+            self_term = self_term or device.self_term
+            kv = kv or device.kvectors
+            kmin = kmin or device.kmin_table
+            cellsort = cellsort or device.cell_sort
         fws = list(fws)
         if not fws:
             raise ArgumentError("FrameworkBatch needs at least one framework")
@@ -144,7 +155,7 @@ class FrameworkBatch:
         k_offsets = [0]
         constant_offset, halfranges = [], []
         ncells, cell_offsets, cellgrid_offsets = [], [], [0]
-        kmin = []
+        kmin_list = []
         offset_parts = []  # per framework: (KE (self + excl + net), self-term mean, type counts, V)
         natoms_total = 0
         for n, fw in enumerate(unique, start=1):
@@ -157,7 +168,7 @@ class FrameworkBatch:
             n_grid = grid_dims(L, w)
             pos = cartesian(fw)
             ty = o2c_arr[ty_orig[n - 1]]
-            perm, local = cell_sort(fw.frac, n_grid)
+            perm, local = (cellsort or cell_sort)(fw.frac, n_grid)
             positions.append(pos[perm])
             types.append(ty[perm])
             charges.append(fw.charges[perm])
@@ -173,7 +184,7 @@ class FrameworkBatch:
             volumes.append(V)
             alphas.append(alpha)
             if not neutral or fw.replication != (1, 1, 1):
-                kv_full, kpref_full, Sh_full, coeffs = full_ktables(A, pos, fw.charges, alpha, kmax, sk)
+                kv_full, kpref_full, Sh_full, coeffs = full_ktables(A, pos, fw.charges, alpha, kmax, sk, kv)
                 if fw.replication != (1, 1, 1):
                     verify_replication(n, fw, kv_full, coeffs, Sh_full)
             self_mean = 0.0
@@ -205,7 +216,7 @@ class FrameworkBatch:
             else:
                 halfranges.append(0.0)
             k_offsets.append(k_offsets[-1] + (len(ks[-1]) if (not neutral) else 0))
-            kmin.append(kmin_table(guest.charges, types[-1], charges[-1], ntypes).reshape(-1))
+            kmin_list.append((kmin or kmin_table)(guest.charges, types[-1], charges[-1], ntypes).reshape(-1))
             counts = np.bincount(ty_orig[n - 1] - 1, minlength=nff)
             self_e = -alpha / math.sqrt(math.pi) * float(np.sum(guest.charges ** 2))
             excl = 0.0
@@ -244,7 +255,7 @@ class FrameworkBatch:
         self.guest_types_orig = np.asarray(guest.types, dtype=np.int64).copy()
         self.guest_sites_orig = guest.sites.copy()
         self.guest_charges_orig = guest.charges.copy()
-        self.kmin = np.concatenate(kmin) if kmin else np.zeros(0)
+        self.kmin = np.concatenate(kmin_list) if kmin_list else np.zeros(0)
         self.cutoff = float(ff.cutoff)
         self.ewald_cutoff = float(ewald.cutoff)
         self.fullk = bool(fullk)

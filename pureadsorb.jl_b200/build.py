@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "pa_capi.cu")
 OUT = os.path.join(HERE, "libpureadsorb_b200.so")
-DEPS = ["pa_capi.cu", "pa_kernels.cuh", "pa_energy32.cuh", "pa_grad32.cuh", "pa_chain32.cuh", "pa_common.cuh",
+DEPS = ["pa_capi.cu", "pa_kernels.cuh", "pa_energy32.cuh", "pa_grad32.cuh", "pa_chain32.cuh", "pa_build.cuh", "pa_common.cuh",
         "pa_coeffs.h"]
 
 

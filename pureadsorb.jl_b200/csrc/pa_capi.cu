@@ -81,6 +81,8 @@ struct pa_context {
     DevMem item_pq;
     // insertion into a loaded configuration: per-call tables and the guest-guest term
     DevMem chain_kS2, chain_const, chain_goff, chain_gsites, chain_gtype, chain_cells, dUg, chain_ksplit;
+    DevMem rj_in, rj_out;                   // pa_batch_rejection_tables: inputs, rho2
+    std::vector<unsigned char> up_rj_in;
     std::vector<unsigned char> up_chain_ksplit;
     std::vector<double> up_chain_kS2, up_chain_const, up_chain_gsites, up_chain_cells;
     std::vector<int32_t> up_chain_goff, up_chain_gtype;
@@ -144,6 +146,8 @@ struct pa_batch {
     std::vector<int32_t> kn_h;         // 3*nk integer coefficients
     std::vector<int32_t> kstep_h;      // nfw: row step in n3
     double guest_qabs = 0;             // Σ |guest charge|
+    std::vector<int32_t> ncells_h;     // 3*nfw cell-list grid
+    std::vector<double> const_offset_h;  // nfw constant offsets (pair-table updates included)
     double cutoff = 0;                 // LJ cutoff
     const double* q64 = nullptr;       // FP64 charges of the stored atoms (inside the arena)
     const int32_t* types0 = nullptr;   // 0-based types (inside the arena)
@@ -241,6 +245,35 @@ void perpendicular_lengths(const double* A, double* L) {
     L[0] = V / norm(c);
     cross(A + 0, A + 6, c); L[1] = V / norm(c);
     cross(A + 0, A + 3, c); L[2] = V / norm(c);
+}
+
+// theta_F(Float64): the smallest theta with exp(-theta) == 0 in FP64, by bisection on the float
+// grid (src/reject.jl:11-19)
+double theta_f64() {
+    static double theta = [] {
+        double lo = 0, hi = 2000;
+        while (std::nextafter(lo, hi) != hi) {
+            double mid = lo + (hi - lo) / 2;
+            if (std::exp(-mid) == 0.0) hi = mid; else lo = mid;
+        }
+        return hi;
+    }();
+    return theta;
+}
+
+// A system's rejection margin (src/widom.jl:202-253): (theta + 2) kT + safety + B_s - c_s with
+// safety = 2 n eps_F (B_s + |c_s|) + 4e-6 B_s, n = N natoms + nk + 8; infinite for infinite B_s.
+double rejection_margin(double Bs, double cs, double natoms, double nk, int N, double eps_F, double theta, double kT) {
+    const double n = N * natoms + nk + 8;
+    const double safety = 2 * n * eps_F * (Bs + std::fabs(cs)) + 4.0e-6 * Bs;
+    return std::isinf(Bs) ? INFINITY : (theta + 2) * kT + safety + Bs - cs;
+}
+
+// The phase-0 stencil half-widths of a system from its largest squared rejection radius.
+void stencil_reach0(const double* cell, const int32_t* ncells, double rmax2, int32_t* reach0) {
+    double L[3];
+    perpendicular_lengths(cell, L);
+    for (int r = 0; r < 3; ++r) reach0[r] = int32_t(std::ceil(std::sqrt(rmax2) * ncells[r] / L[r]));
 }
 
 std::vector<int64_t> system_counts(int64_t ninsert, int64_t nsys, int64_t run) {
@@ -888,6 +921,7 @@ pa_status set_pair_tables_impl(pa_context* ctx, pa_batch* B, const double* sigma
                                  cudaMemcpyHostToDevice, st));
     PA_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(d.const_offset), constant_offset, sizeof(double) * B->nfw,
                                  cudaMemcpyHostToDevice, st));
+    B->const_offset_h.assign(constant_offset, constant_offset + B->nfw);
     return wait_stream(ctx);
 }
 
@@ -1044,6 +1078,8 @@ pa_status pa_batch_upload(pa_context* ctx, const pa_batch_desc* desc, int32_t pr
         B->guest_q.push_back(desc->guest_charges[a]);
     }
     B->cutoff = desc->cutoff;
+    B->ncells_h.assign(desc->ncells, desc->ncells + 3 * nfw);
+    B->const_offset_h.assign(desc->constant_offset, desc->constant_offset + nfw);
     B->recip_bound.assign(nfw, 0.0);
     for (int f = 0; f < nfw; ++f)
         for (int32_t i = desc->k_offsets[f]; i < desc->k_offsets[f + 1]; ++i)
@@ -1758,6 +1794,164 @@ pa_status pa_structure_factor(pa_context* ctx, const double* ks, int64_t nk, con
     return wait_stream(ctx);
 }
 
+pa_status pa_batch_rejection_tables(pa_context* ctx, const pa_batch* B, const double* bs, const double* kmin, double kT,
+                                    double eps_F, double* rho2, int32_t* reach0, int32_t* bad_system) {
+    if (!ctx || !B || !bs || !kmin || !rho2 || !reach0) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (B->ctx != ctx) return fail(ctx, PA_ERR_STATE, "batch was uploaded on another context");
+    if (bad_system) *bad_system = 0;
+    const int nsys = B->nsys, N = B->nguest, nt = B->ntypes, nfw = B->nfw;
+    const double theta = theta_f64();
+    // the systems' margins on the host (as pa_rejection_tables forms them), the root searches on
+    // the device, the reaches on the host
+    std::vector<double> margin(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        const int fw = B->framework_of[s] - 1;
+        margin[s] = rejection_margin(bs[fw], B->const_offset_h[fw], B->atom_offsets[fw + 1] - B->atom_offsets[fw],
+                                     B->k_offsets[fw + 1] - B->k_offsets[fw], N, eps_F, theta, kT);
+        if (!(margin[s] > 0)) {
+            if (bad_system) *bad_system = s + 1;
+            return fail(ctx, PA_ERR_ARG, "system " + std::to_string(s + 1) + ": rejection margin is not positive");
+        }
+    }
+    const int64_t nr = int64_t(nsys) * N * nt, nq = int64_t(N) * nt, nkm = int64_t(nfw) * N * nt;
+    // one packed upload: margins, (site, type) sigma and epsilon, kmin
+    std::vector<unsigned char> img(sizeof(double) * (nsys + 2 * nq + nkm));
+    double* ip = reinterpret_cast<double*>(img.data());
+    std::memcpy(ip, margin.data(), sizeof(double) * nsys);
+    std::memcpy(ip + nsys, B->site_sigma.data(), sizeof(double) * nq);
+    std::memcpy(ip + nsys + nq, B->site_eps.data(), sizeof(double) * nq);
+    std::memcpy(ip + nsys + 2 * nq, kmin, sizeof(double) * nkm);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    PA_CUDA(ctx, upload_cached(ctx->rj_in, ctx->up_rj_in, img, st));
+    PA_CUDA(ctx, ctx->rj_out.ensure(sizeof(double) * std::max<int64_t>(1, nr)));
+    const double* d = ctx->rj_in.as<double>();
+    const int32_t* fwo = B->precision == PA_PRECISION_F32 ? B->d32.framework_of : B->d64.framework_of;
+    if (nr > 0) {
+        pa::k_rho2<<<unsigned((nr + 255) / 256), 256, 0, st>>>(d + nsys, d + nsys + nq, d + nsys + 2 * nq, d, fwo, nsys,
+                                                                N, nt, B->cutoff, ctx->rj_out.as<double>());
+        PA_CUDA(ctx, cudaGetLastError());
+        PA_CUDA(ctx, cudaMemcpyAsync(rho2, ctx->rj_out.p, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
+    }
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    for (int s = 0; s < nsys; ++s) {
+        const int fw = B->framework_of[s] - 1;
+        double rmax = 0;
+        for (int64_t q = 0; q < nq; ++q) {
+            const double r2 = rho2[int64_t(s) * nq + q];
+            if (r2 < 0) {
+                if (bad_system) *bad_system = s + 1;
+                return fail(ctx, PA_ERR_ARG, "system " + std::to_string(s + 1) + ": a rejection-radius search failed");
+            }
+            rmax = std::max(rmax, r2);
+        }
+        stencil_reach0(B->cells_h.data() + 9 * fw, B->ncells_h.data() + 3 * fw, rmax, reach0 + 3 * s);
+    }
+    return PA_OK;
+}
+
+pa_status pa_kvectors(pa_context* ctx, const double* B9, const int32_t* nmax, double kmax, double c2piv, double four_a2,
+                      int64_t capacity, double* ks, double* weights, double* kpref, int32_t* coeffs, int64_t* nk) {
+    if (!ctx || !B9 || !nmax || !nk) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (!(kmax >= 0) || !std::isfinite(kmax)) return fail(ctx, PA_ERR_ARG, "kmax must be finite and >= 0");
+    for (int r = 0; r < 3; ++r)
+        if (nmax[r] < 0 || nmax[r] > 4096) return fail(ctx, PA_ERR_ARG, "nmax out of range [0, 4096]");
+    const int64_t M = (int64_t(nmax[0]) + 1) * (2 * int64_t(nmax[1]) + 1) * (2 * int64_t(nmax[2]) + 1);
+    if (capacity < M - 1) return fail(ctx, PA_ERR_ARG, "capacity below the candidate count (n0+1)(2n1+1)(2n2+1)-1");
+    if (M > (int64_t(1) << 30)) return fail(ctx, PA_ERR_ARG, "too many candidate k-vectors");
+    if (M - 1 > 0 && (!ks || !weights || !kpref || !coeffs)) return fail(ctx, PA_ERR_ARG, "null output array");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    DevMem dks, dw, dkp, dc, dn;
+    PA_CUDA(ctx, dks.ensure(sizeof(double) * 3 * M));
+    PA_CUDA(ctx, dw.ensure(sizeof(double) * M));
+    PA_CUDA(ctx, dkp.ensure(sizeof(double) * M));
+    PA_CUDA(ctx, dc.ensure(sizeof(int32_t) * 3 * M));
+    PA_CUDA(ctx, dn.ensure(sizeof(int32_t)));
+    pa::KvecArgs g{};
+    for (int r = 0; r < 9; ++r) g.B[r] = B9[r];
+    for (int r = 0; r < 3; ++r) g.n[r] = nmax[r];
+    g.kmax = kmax; g.c2piv = c2piv; g.four_a2 = four_a2;
+    g.ks = dks.as<double>(); g.w = dw.as<double>(); g.kpref = dkp.as<double>(); g.coeffs = dc.as<int32_t>();
+    g.count = dn.as<int32_t>();
+    pa::k_kvectors<<<1, 1024, 0, st>>>(g);
+    PA_CUDA(ctx, cudaGetLastError());
+    int32_t count = 0;
+    PA_CUDA(ctx, cudaMemcpyAsync(&count, dn.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    pa_status ws = wait_stream(ctx);
+    if (ws != PA_OK) return ws;
+    *nk = count;
+    if (count > 0) {
+        PA_CUDA(ctx, cudaMemcpyAsync(ks, dks.p, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(weights, dw.p, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(kpref, dkp.p, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+        PA_CUDA(ctx, cudaMemcpyAsync(coeffs, dc.p, sizeof(int32_t) * 3 * count, cudaMemcpyDeviceToHost, st));
+    }
+    return wait_stream(ctx);
+}
+
+pa_status pa_kmin_table(pa_context* ctx, const double* guest_charges, int32_t nguest, const int32_t* types,
+                        const double* charges, int64_t natoms, int32_t ntypes, double* kmin) {
+    if (!ctx || !kmin || (nguest > 0 && !guest_charges) || (natoms > 0 && (!types || !charges)))
+        return fail(ctx, PA_ERR_ARG, "null argument");
+    if (nguest < 0 || ntypes < 1 || natoms < 0) return fail(ctx, PA_ERR_ARG, "invalid sizes");
+    for (int64_t h = 0; h < natoms; ++h)
+        if (types[h] < 1 || types[h] > ntypes) return fail(ctx, PA_ERR_ARG, "atom type out of range [1, ntypes]");
+    const int64_t nq = int64_t(nguest) * ntypes;
+    if (nq == 0) return PA_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    DevMem dg, dt, dq, dk;
+    std::vector<double> vg(guest_charges, guest_charges + nguest), vq(charges, charges + natoms);
+    std::vector<int32_t> vt(types, types + natoms);
+    PA_CUDA(ctx, upload(dg, vg, st));
+    PA_CUDA(ctx, upload(dt, vt, st));
+    PA_CUDA(ctx, upload(dq, vq, st));
+    PA_CUDA(ctx, dk.ensure(sizeof(double) * nq));
+    PA_CUDA(ctx, cudaMemsetAsync(dk.p, 0, sizeof(double) * nq, st));
+    if (natoms > 0) {
+        const unsigned grid = unsigned(std::min<int64_t>((natoms + 255) / 256, int64_t(ctx->num_sms) * 8));
+        pa::k_kmin<<<grid, 256, 0, st>>>(dg.as<double>(), nguest, dt.as<int32_t>(), dq.as<double>(), natoms, ntypes,
+                                         dk.as<unsigned long long>());
+        PA_CUDA(ctx, cudaGetLastError());
+    }
+    PA_CUDA(ctx, cudaMemcpyAsync(kmin, dk.p, sizeof(double) * nq, cudaMemcpyDeviceToHost, st));
+    return wait_stream(ctx);
+}
+
+pa_status pa_cell_sort(pa_context* ctx, const double* frac, int64_t natoms, const int32_t* ncells, int64_t* perm,
+                       int32_t* offsets) {
+    if (!ctx || !ncells || !offsets || (natoms > 0 && (!frac || !perm))) return fail(ctx, PA_ERR_ARG, "null argument");
+    if (natoms < 0 || natoms > INT32_MAX) return fail(ctx, PA_ERR_ARG, "natoms out of range");
+    for (int r = 0; r < 3; ++r)
+        if (ncells[r] < 1) return fail(ctx, PA_ERR_ARG, "ncells must be >= 1");
+    const int64_t ncell = int64_t(ncells[0]) * ncells[1] * ncells[2];
+    if (ncell > INT32_MAX / 2) return fail(ctx, PA_ERR_ARG, "too many cells");
+    for (int64_t i = 0; i < 3 * natoms; ++i)
+        if (!std::isfinite(frac[i])) return fail(ctx, PA_ERR_ARG, "fractional coordinates must be finite");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = ctx->stream;
+    DevMem df, dci, dcnt, doff, dcur, dperm;
+    std::vector<double> vf(frac, frac + 3 * natoms);
+    PA_CUDA(ctx, upload(df, vf, st));
+    PA_CUDA(ctx, dci.ensure(sizeof(int32_t) * std::max<int64_t>(1, natoms)));
+    PA_CUDA(ctx, dcnt.ensure(sizeof(int32_t) * ncell));
+    PA_CUDA(ctx, doff.ensure(sizeof(int32_t) * (ncell + 1)));
+    PA_CUDA(ctx, dcur.ensure(sizeof(int32_t) * ncell));
+    PA_CUDA(ctx, dperm.ensure(sizeof(int64_t) * std::max<int64_t>(1, natoms)));
+    PA_CUDA(ctx, cudaMemsetAsync(dcnt.p, 0, sizeof(int32_t) * ncell, st));
+    if (natoms > 0)
+        pa::k_cell_count<<<unsigned((natoms + 255) / 256), 256, 0, st>>>(df.as<double>(), natoms, ncells[0], ncells[1],
+                                                                         ncells[2], dci.as<int32_t>(), dcnt.as<int32_t>());
+    pa::k_cell_offsets<<<1, 1024, 0, st>>>(dcnt.as<int32_t>(), int32_t(ncell), doff.as<int32_t>(), dcur.as<int32_t>());
+    if (natoms > 0) pa::k_cell_place<<<1, 32, 0, st>>>(dci.as<int32_t>(), natoms, dcur.as<int32_t>(), dperm.as<int64_t>());
+    PA_CUDA(ctx, cudaGetLastError());
+    if (natoms > 0) PA_CUDA(ctx, cudaMemcpyAsync(perm, dperm.p, sizeof(int64_t) * natoms, cudaMemcpyDeviceToHost, st));
+    PA_CUDA(ctx, cudaMemcpyAsync(offsets, doff.p, sizeof(int32_t) * (ncell + 1), cudaMemcpyDeviceToHost, st));
+    return wait_stream(ctx);
+}
+
 }  // extern "C"
 
 // =============================================================================================
@@ -2012,47 +2206,9 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
 
 // =============================================================================================
 // Host: rejection radii and phase-0 stencil reaches of one call (build_rejection_tables,
-// src/widom.jl:202-253; find_rho2, src/reject.jl:168-209; theta_F, src/reject.jl:11-19).
+// src/widom.jl:202-253; find_rho2, src/reject.jl:168-209; theta_F, src/reject.jl:11-19). The root
+// search is pa::rho2_search, the same sequence pa_batch_rejection_tables runs on the device.
 // =============================================================================================
-namespace {
-
-double theta_f64() {
-    static double theta = [] {
-        double lo = 0, hi = 2000;
-        while (std::nextafter(lo, hi) != hi) {
-            double mid = lo + (hi - lo) / 2;
-            if (std::exp(-mid) == 0.0) hi = mid; else lo = mid;
-        }
-        return hi;
-    }();
-    return theta;
-}
-
-inline double lj4(double r2, double s, double e) { double x = s * s / r2; x = x * x * x; return 4 * e * (x * x - x); }
-
-// first root of LJ(r) - |kmin|/r = margin scanning up from r -> 0, clamped to r_lj; 0 for an
-// infinite margin or a zero epsilon; -1 when a search exceeds its iteration cap
-double rho2_of(double s, double e, double kmin, double margin, double r_lj) {
-    if (std::isinf(margin) || e == 0) return 0;
-    auto f = [&](double r) { return lj4(r * r, s, e) - std::fabs(kmin) / r - margin; };
-    const int cap = 200;
-    const double eps = 2.220446049250313e-16;
-    double hi = s; int it = 0;
-    while (f(hi) >= 0) { hi *= 2; if (++it > cap) return -1; }
-    double lo = hi; it = 0;
-    while (f(lo) < 0) { lo /= 2; if (++it > cap) return -1; }
-    it = 0;
-    while (hi - lo > 4 * eps * hi) {
-        double mid = (lo + hi) / 2;
-        if (f(mid) > 0) lo = mid; else hi = mid;
-        if (++it > cap) return -1;
-    }
-    double r = std::min((lo + hi) / 2, r_lj);
-    return r * r;
-}
-
-}  // namespace
-
 extern "C" pa_status pa_rejection_tables(const pa_batch_desc* d, const double* bs, const double* kmin, double kT,
                                          double eps_F, double* rho2, int32_t* reach0, int32_t* bad_system) {
     if (!d || !bs || !kmin || !rho2 || !reach0) return PA_ERR_ARG;
@@ -2061,25 +2217,20 @@ extern "C" pa_status pa_rejection_tables(const pa_batch_desc* d, const double* b
     const double theta = theta_f64();
     for (int s = 0; s < d->nsys; ++s) {
         const int fw = d->framework_of[s] - 1;
-        const double Bs = bs[fw], cs = d->constant_offset[fw];
-        const double natoms = d->atom_offsets[fw + 1] - d->atom_offsets[fw], nk = d->k_offsets[fw + 1] - d->k_offsets[fw];
-        const double n = N * natoms + nk + 8;
-        const double safety = 2 * n * eps_F * (Bs + std::fabs(cs)) + 4.0e-6 * Bs;
-        const double margin = std::isinf(Bs) ? INFINITY : (theta + 2) * kT + safety + Bs - cs;
+        const double margin = rejection_margin(bs[fw], d->constant_offset[fw], d->atom_offsets[fw + 1] - d->atom_offsets[fw],
+                                               d->k_offsets[fw + 1] - d->k_offsets[fw], N, eps_F, theta, kT);
         if (!(margin > 0)) { if (bad_system) *bad_system = s + 1; return PA_ERR_ARG; }
         double rmax = 0;
         for (int a = 0; a < N; ++a)
             for (int t = 0; t < nt; ++t) {
                 const int gt = d->guest_types[a] - 1;
-                const double r2 = rho2_of(d->sigma[gt + nt * t], d->epsilon[gt + nt * t],
-                                          kmin[int64_t(fw) * N * nt + a * nt + t], margin, d->cutoff);
+                const double r2 = pa::rho2_search(d->sigma[gt + nt * t], d->epsilon[gt + nt * t],
+                                                  kmin[int64_t(fw) * N * nt + a * nt + t], margin, d->cutoff);
                 if (r2 < 0) { if (bad_system) *bad_system = s + 1; return PA_ERR_ARG; }
                 rho2[int64_t(s) * N * nt + a * nt + t] = r2;
                 rmax = std::max(rmax, r2);
             }
-        double L[3];
-        perpendicular_lengths(d->cells + 9 * fw, L);
-        for (int r = 0; r < 3; ++r) reach0[3 * s + r] = int32_t(std::ceil(std::sqrt(rmax) * d->ncells[3 * fw + r] / L[r]));
+        stencil_reach0(d->cells + 9 * fw, d->ncells + 3 * fw, rmax, reach0 + 3 * s);
     }
     return PA_OK;
 }

@@ -104,6 +104,13 @@ template <> struct St<double> {
         return std::fma(a, b, c);
 #endif
     }
+    static PA_HD double div(double a, double b) {
+#ifdef __CUDA_ARCH__
+        return __ddiv_rn(a, b);
+#else
+        return a / b;
+#endif
+    }
     static PA_HD double sqrt(double a) {
 #ifdef __CUDA_ARCH__
         return __dsqrt_rn(a);

@@ -866,6 +866,7 @@ __device__ __forceinline__ float erfc_over_r(float r2, float alpha) {
 #include "pa_energy32.cuh"
 #include "pa_grad32.cuh"
 #include "pa_chain32.cuh"
+#include "pa_build.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // k_energy64: the plain FP64 form of the reference algorithm (src/energy.jl:42-82): for every

@@ -46,20 +46,34 @@ def pk(k2, alpha, V):
     return 2 * math.pi / V * np.exp(-np.asarray(k2) / (4 * alpha**2)) / np.asarray(k2)
 
 
+def kvector_bounds(A, kmax):
+    """|n_i| <= kmax |a_i| / 2 pi for the half-space enumeration (src/ewald.jl:143)."""
+    return np.array([int(math.ceil(kmax * np.linalg.norm(A[:, i]) / (2 * math.pi))) for i in range(3)], dtype=np.int32)
+
+
 def kvectors(A, kmax):
     """Half-space k-vectors within kmax: n1 >= 0, weight 2 when n1 > 0, in the order n1, n2, n3
-    (n3 fastest). Returns (ks (nk,3), weights, integer coefficients (nk,3)) (src/ewald.jl:142-157)."""
+    (n3 fastest). Returns (ks (nk,3), weights, integer coefficients (nk,3)) (src/ewald.jl:142-157).
+    k = (n1 B[:,0] + n2 B[:,1]) + n3 B[:,2] and |k| = sqrt((kx^2 + ky^2) + kz^2), in that operation
+    order (pa_kvectors forms them the same way on the device)."""
     B = reciprocal_basis(A)
-    n = [int(math.ceil(kmax * np.linalg.norm(A[:, i]) / (2 * math.pi))) for i in range(3)]
+    n = kvector_bounds(A, kmax)
     n1, n2, n3 = np.meshgrid(np.arange(0, n[0] + 1), np.arange(-n[1], n[1] + 1), np.arange(-n[2], n[2] + 1),
                              indexing="ij")
     c = np.stack([n1.ravel(), n2.ravel(), n3.ravel()], axis=1)
     c = c[np.any(c != 0, axis=1)]
-    k = c.astype(np.float64) @ B.T
-    keep = np.linalg.norm(k, axis=1) <= kmax
+    cf = c.astype(np.float64)
+    k = (cf[:, 0:1] * B[:, 0] + cf[:, 1:2] * B[:, 1]) + cf[:, 2:3] * B[:, 2]
+    keep = np.sqrt(k2_of(k)) <= kmax
     c, k = c[keep], k[keep]
     w = np.where(c[:, 0] == 0, 1.0, 2.0)
     return k, w, c.astype(np.int32)
+
+
+def k2_of(k):
+    """|k|^2 = (kx^2 + ky^2) + kz^2 per row."""
+    k = np.asarray(k, dtype=np.float64).reshape(-1, 3)
+    return (k[:, 0] * k[:, 0] + k[:, 1] * k[:, 1]) + k[:, 2] * k[:, 2]
 
 
 def structure_factor(ks, positions, charges, chunk_elems=1 << 22):
@@ -77,12 +91,17 @@ def structure_factor(ks, positions, charges, chunk_elems=1 << 22):
     return S
 
 
-def full_ktables(A, positions, charges, alpha, kmax, sk=None):
+def full_ktables(A, positions, charges, alpha, kmax, sk=None, kv=None):
     """Every k-vector kvectors enumerates with its prefactor, host structure factor and integer
     coefficients (src/reference.jl:10-16). `sk`, if given, computes the structure factor
-    (ks, positions, charges) -> complex array (e.g. on the device)."""
-    ks, w, coeffs = kvectors(A, kmax)
+    (ks, positions, charges) -> complex array (e.g. on the device); `kv`, if given, the k-vectors
+    and prefactors (B, nmax, kmax, alpha, V) -> (ks, weights, kpref, coefficients) (e.g. on the
+    device, Context.kvectors)."""
     V = volume(A)
-    kpref = w * pk(np.sum(ks * ks, axis=1), alpha, V) if len(ks) else np.zeros(0)
+    if kv is not None:
+        ks, w, kpref, coeffs = kv(reciprocal_basis(A), kvector_bounds(A, kmax), kmax, alpha, V)
+    else:
+        ks, w, coeffs = kvectors(A, kmax)
+        kpref = w * pk(k2_of(ks), alpha, V) if len(ks) else np.zeros(0)
     S = (sk or structure_factor)(ks, positions, charges)
     return ks, kpref, S, coeffs

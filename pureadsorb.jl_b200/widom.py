@@ -58,28 +58,35 @@ def boltzmann_weight(dU, kT):
     return w, (0.0 if w == 0 else dU64 * w)
 
 
-def build_rejection_tables(batch, kT):
+def build_rejection_tables(batch, kT, ctx=None):
     """Rejection radii rho2 (nsys*N*ntypes) and phase-0 stencil half-widths reach0 (nsys x 3) for
-    one call (src/widom.jl:202-253), computed by the library's host code (pa_rejection_tables).
-    The summation-error term uses eps of the batch's float type; theta is theta_F(Float64)
-    because weights accumulate in FP64. Cached on the batch per (kT, eps)."""
+    one call (src/widom.jl:202-253), computed by the library's host code (pa_rejection_tables),
+    or, given a context, with the root searches on the device through the batch's upload to it
+    (pa_batch_rejection_tables; the same values bit for bit). The summation-error term uses eps of
+    the batch's float type; theta is theta_F(Float64) because weights accumulate in FP64. Cached
+    on the batch per (kT, eps)."""
     key = (float(kT), float(np.finfo(batch.T).eps))
     cache = getattr(batch, "_rejection", None)
     if cache is not None and key in cache:
         return cache[key]
     N = len(batch.guest_types)
     nt = len(batch.sigma)
-    d, keep = batch.desc()
     bs = np.ascontiguousarray(batch.bs, dtype=np.float64)
     kmin = np.ascontiguousarray(batch.kmin, dtype=np.float64)
-    rho2 = np.zeros(batch.nsys * N * nt)
-    reach0 = np.zeros((batch.nsys, 3), dtype=np.int32)
-    bad = _lib.ctypes.c_int32(0)
-    st = _lib.lib().pa_rejection_tables(_lib.ctypes.byref(d), _lib.ptr(bs), _lib.ptr(kmin), float(kT),
-                                        float(np.finfo(batch.T).eps), _lib.ptr(rho2), _lib.ptr(reach0),
-                                        _lib.ctypes.byref(bad))
+    eps_F = float(np.finfo(batch.T).eps)
+    if ctx is not None:
+        rho2, reach0, bad_s = batch.device(ctx).rejection_tables(bs, kmin, kT, eps_F, batch.nsys, N, nt)
+        st = _lib.PA_OK if bad_s == 0 else _lib.PA_ERR_ARG
+    else:
+        d, keep = batch.desc()
+        rho2 = np.zeros(batch.nsys * N * nt)
+        reach0 = np.zeros((batch.nsys, 3), dtype=np.int32)
+        bad = _lib.ctypes.c_int32(0)
+        st = _lib.lib().pa_rejection_tables(_lib.ctypes.byref(d), _lib.ptr(bs), _lib.ptr(kmin), float(kT), eps_F,
+                                            _lib.ptr(rho2), _lib.ptr(reach0), _lib.ctypes.byref(bad))
+        bad_s = bad.value
     if st != _lib.PA_OK:
-        s = bad.value
+        s = bad_s
         raise ArgumentError(f"build_rejection_tables: system {s} has no valid rejection radius (margin <= 0 or a "
                             f"root search failed; kT={kT}, theta_F={float(theta_F(np.float64))})")
     rho2.flags.writeable = False
@@ -152,10 +159,13 @@ def _reduce_rows(sW, sUW, n, kT, V, first=1):
 
 class B200Backend:
     """The device `backend` of widom: one CUDA device context of the library. Plays the role of
-    the KernelAbstractions backend object the reference takes (src/widom.jl:298-301)."""
+    the KernelAbstractions backend object the reference takes (src/widom.jl:298-301). With
+    device_tables=True each call's rejection radii are computed on the device
+    (pa_batch_rejection_tables, equal to the host's), which pays off for batches of many systems."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, device_tables=False):
         self.device = device
+        self.device_tables = bool(device_tables)
         self._ctx = None
 
     @property
@@ -219,7 +229,8 @@ def _widom(batch, guest, *, reject, T, ninsert, backend=None, seed=0, chunk=2**1
     backend = backend or default_backend()
     ctx = backend.ctx
     dev = batch.device(ctx)
-    rho2, reach0 = build_rejection_tables(batch, kT) if reject else (None, None)
+    rho2, reach0 = (build_rejection_tables(batch, kT, ctx if getattr(backend, "device_tables", False) else None)
+                    if reject else (None, None))
     rho2c = None if rho2 is None else np.ascontiguousarray(rho2)
     reach0c = None if reach0 is None else np.ascontiguousarray(reach0.reshape(-1))
     args = _lib.WidomArgs()
