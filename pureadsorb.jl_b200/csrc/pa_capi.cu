@@ -802,33 +802,18 @@ void launch_pose(const pa_batch* B, const pa::CallArgs& ca, const pa::Work& w, c
     pa::k_pose<F, NS><<<grid, 256, 0, st>>>(d, ca, w, rho2, reach0);
 }
 
-// Raises the energy kernel's dynamic shared-memory limit when the batch's type tables need it
-// (a function attribute, set before any stream capture).
-template <int NS>
-cudaError_t prepare_energy(const pa_batch* B) {
-    if (B->precision != PA_PRECISION_F32) return cudaSuccess;
-    const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
-    if (dyn <= 48 * 1024) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(pa::k_energy32<NS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(pa::k_energy32<NS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
-    return e;
-}
-
 template <int NS>
 cudaError_t launch_energy(const pa_batch* B, const pa::DevBatch<float>& v32, const pa::CallArgs& ca, const pa::Work& w,
                           int32_t num_sms, int32_t ctas, cudaStream_t st) {
     if (B->precision == PA_PRECISION_F32) {
-        const size_t dyn = sizeof(float) * 2 * NS * size_t(B->ntypes);
         const int32_t per = (ctas >= 1 && ctas <= PA_CTAS_PER_SM32) ? ctas : PA_CTAS_PER_SM32;
         const unsigned grid = unsigned(num_sms * per), block = 32 * PA_WARPS32;
         if (v32.rl2 == v32.re2) {
-            if (w.item_pq) pa::k_energy32<NS, true, true><<<grid, block, dyn, st>>>(v32, ca, w);
-            else pa::k_energy32<NS, true, false><<<grid, block, dyn, st>>>(v32, ca, w);
+            if (w.item_pq) pa::k_energy32<NS, true, true><<<grid, block, 0, st>>>(v32, ca, w);
+            else pa::k_energy32<NS, true, false><<<grid, block, 0, st>>>(v32, ca, w);
         } else {
-            if (w.item_pq) pa::k_energy32<NS, false, true><<<grid, block, dyn, st>>>(v32, ca, w);
-            else pa::k_energy32<NS, false, false><<<grid, block, dyn, st>>>(v32, ca, w);
+            if (w.item_pq) pa::k_energy32<NS, false, true><<<grid, block, 0, st>>>(v32, ca, w);
+            else pa::k_energy32<NS, false, false><<<grid, block, 0, st>>>(v32, ca, w);
         }
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
@@ -1389,11 +1374,6 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     ca.seed_dev = ctx->scal.as<uint64_t>(); ca.kT_dev = ctx->scal.as<double>() + 1;
     ca.k_offset = chain ? chain->k_offset : 0; ca.koff_dev = reinterpret_cast<const int64_t*>(ctx->scal.as<double>() + 2);
     ca.rho2max = args->reject ? ctx->rho2max.p : nullptr;
-    {
-        cudaError_t e = cudaSuccess;
-        PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
-        if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel attributes: ") + cudaGetErrorString(e));
-    }
     const int32_t ctas = ctx->tuning.ctas_per_sm;
     // the device sequence of one call: memsets, pose + phase 0, scan, scatter, energy, segment
     // sums, and the copies of the segment sums and counters into pinned host memory
@@ -2175,7 +2155,6 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
     PA_CUDA(ctx, cudaGetLastError());
     {
         cudaError_t e = cudaSuccess;
-        PA_DISPATCH_NS(N, (e = prepare_energy<NSV>(B)));
         pa::DevBatch<float> v32;  // the context's FP32/FP64 pair split, as pa_widom applies it
         std::memcpy(&v32, &B->d32, sizeof(v32));
         apply_split(ctx, v32);

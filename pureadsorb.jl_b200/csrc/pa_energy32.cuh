@@ -34,18 +34,32 @@ __device__ __forceinline__ float ex2_ftz(float x) {
     return r;
 }
 
-// erfc(alpha r) / r in FP64 from r^2 and 1/r: 1/r - alpha S(alpha^2 r^2), S(u) = erf(sqrt u)/sqrt u
-// as a polynomial in u (PA_ERFS64, alpha r <= 2, relative error of erfc below 2e-13); CUDA's
-// double erfc beyond that.
+// 1/sqrt(x) in FP64, x > 0 and normal: the hardware approximation (rsqrt.approx.ftz.f64) refined
+// by two steps of Newton's iteration y <- y (3/2 - (x/2) y^2), each of which squares the relative
+// error; a few ulp from 1/sqrt(x).
+__device__ __forceinline__ double rsqrt64(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    y = y * fma(-h * y, y, 1.5);
+    return y;
+}
+
+// S(u) = erf(sqrt u)/sqrt u on 0 <= u <= PA_ERFS64_UMAX from the PA_ERFS64 polynomial (Horner).
+__device__ __forceinline__ double erfs64(double u) {
+    const double c[PA_NERFS64] = PA_ERFS64_INIT;
+    double p = c[PA_NERFS64 - 1];
+#pragma unroll
+    for (int k = PA_NERFS64 - 2; k >= 0; --k) p = fma(p, u, c[k]);
+    return p;
+}
+
+// erfc(alpha r) / r in FP64 from r^2 and 1/r: 1/r - alpha S(alpha^2 r^2) for alpha r <= 2 (S of
+// degree 13, |error| below 2.4e-13 there); CUDA's double erfc beyond that.
 __device__ __forceinline__ double screened64(double r2, double ri, double alpha) {
     const double u = (alpha * alpha) * r2;
-    if (u <= PA_ERFS64_UMAX) {
-        const double c[PA_NERFS64] = PA_ERFS64_INIT;
-        double p = c[PA_NERFS64 - 1];
-#pragma unroll
-        for (int k = PA_NERFS64 - 2; k >= 0; --k) p = fma(p, u, c[k]);
-        return fma(-alpha, p, ri);
-    }
+    if (u <= PA_ERFS64_UMAX) return fma(-alpha, erfs64(u), ri);
     return erfc(alpha * (r2 * ri)) * ri;
 }
 
@@ -80,27 +94,27 @@ __device__ __forceinline__ void bin_centre(const DevBatch<float>& b, int32_t fw,
     cz = __fdiv_rn(float(bz) + 0.5f, float(nb[2]));
 }
 
-// One pair in FP64 from the FP64 list entry e and the item's FP64 site (relative to the bin
-// centre): the cutoff tests, LJ and the screened Coulomb term (skq = KE times the site charge),
-// added to enear; PQ also adds the pair's x^6(x^6-1) and x^6(2x^6-1) (x = sigma/r) to the run sums.
+// One pair in FP64 from the FP64 list entry e (xyzq64) and the item's FP64 site (relative to the
+// bin centre): the cutoff tests against rl2 and re2, LJ (lj = (sigma^2, 4 eps) of the site and the
+// entry's type) and the screened Coulomb term (skq = KE times the site charge), added to enear; PQ
+// also adds the pair's x^6(x^6-1) and x^6(2x^6-1) (x = sigma/r) to the run sums.
 template <bool PQ>
-__device__ __forceinline__ void pair64(const DevBatch<float>& b, int32_t e, double px, double py, double pz,
-                                       int32_t as, int32_t ty, double skq, int32_t fw, bool charged, double& enear,
+__device__ __forceinline__ void pair64(const double4* xyzq64, double rl2, double re2, int32_t e, double px, double py,
+                                       double pz, double2 lj, double skq, double alpha, bool charged, double& enear,
                                        float& sp, float& sq) {
-    const double4 e64 = b.list_xyzq64[e];
+    const double4 e64 = xyzq64[e];
     const double ex = px - e64.x, ey = py - e64.y, ez = pz - e64.z;
     const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
-    const double rid = rsqrt(r2d);
-    const int32_t nt = b.ntypes;
+    const double rid = rsqrt64(r2d);
     double en = 0.0;
-    if (r2d < b.rl2_64) {
-        const double x = b.sig2_64[as * nt + ty] * (rid * rid);
+    if (r2d < rl2) {
+        const double x = lj.x * (rid * rid);
         const double x3 = x * x * x;
         const double u = x3 * x3 - x3;
-        en = b.eps4_64[as * nt + ty] * u;
+        en = lj.y * u;
         if (PQ) { sp += float(u); sq += float(fma(x3, x3, u)); }
     }
-    if (charged && r2d < b.re2_64) en = fma(skq * e64.w, screened64(r2d, rid, b.alphas[fw]), en);
+    if (charged && r2d < re2) en = fma(skq * e64.w, screened64(r2d, rid, alpha), en);
     enear += en;
 }
 
@@ -114,10 +128,10 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     __shared__ double4 s_site64[NS]; // the same in FP64 (the FP64 pairs)
     __shared__ double2 s_p64[PA_WARPS32][32][2];  // each lane's site in FP64 (x, y | z, -), FP64 pairs
     __shared__ uint32_t s_mk[PA_WARPS32][PA_CHUNK32 / 32][32];  // per lane: the chunk's FP64 entries (bits)
-    extern __shared__ float s_lj[];  // sig2 then eps4, NS*ntypes each
+    // the (site, type) LJ tables stay in global memory (read at type-run boundaries and per FP64
+    // pair, through L1): in shared memory a batch of many host types would cost CTAs per SM
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int nt = b.ntypes;
-    for (int x = tid; x < NS * nt; x += blockDim.x) { s_lj[x] = b.sig2[x]; s_lj[NS * nt + x] = b.eps4[x]; }
     if (tid < NS) {
         s_site[tid] = make_float4(b.gsite[3 * tid], b.gsite[3 * tid + 1], b.gsite[3 * tid + 2],
                                   float(KE * double(b.gq[tid])));
@@ -126,8 +140,6 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
     }
     if (lane == 0) { mbar_init(&s_bar[wp][0], 1); mbar_init(&s_bar[wp][1], 1); mbar_fence_init(); }
     __syncthreads();  // the only CTA-wide barrier: tables and barriers are ready
-    const float* s_sig2 = s_lj;
-    const float* s_eps4 = s_lj + NS * nt;
     float4(*xyzq)[PA_CHUNK32] = s_xyzq[wp];
     uint64_t* bar = s_bar[wp];
     uint32_t gchunk = 0;  // chunks this warp has consumed (selects stage and parity)
@@ -199,7 +211,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         // one run boundary to the next and reloads them there
         const int2* runs = b.list_runs + int64_t(bin) * b.runs_per_bin;
         int32_t ri = 0, rnext = runs[1].x, ty = runs[0].y;
-        float sg = s_sig2[as * nt + ty], ep = s_eps4[as * nt + ty];
+        float sg = __ldg(b.sig2 + as * nt + ty), ep = __ldg(b.eps4 + as * nt + ty);
         // without the adjoint sums: 4 eps ((sigma/r)^12 - (sigma/r)^6) = r^-6 (ljA r^-6 - ljB),
         // ljA = 4 eps sigma^12, ljB = 4 eps sigma^6, one multiplication fewer per pair
         float ljB = ep * (sg * sg * sg), ljA = ljB * (sg * sg * sg);
@@ -234,8 +246,9 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                 // FP64 (the adjoint's form here, every other form after the chunk)
                                 if (PQ) {
                                     const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
-                                    pair64<true>(b, base + j, pxy.x, pxy.y, pzz.x, as, ty, s_site64[as].w, fw, charged,
-                                                 enear, sp, sq);
+                                    pair64<true>(b.list_xyzq64, b.rl2_64, b.re2_64, base + j, pxy.x, pxy.y, pzz.x,
+                                                 make_double2(b.sig2_64[as * nt + ty], b.eps4_64[as * nt + ty]),
+                                                 s_site64[as].w, b.alphas[fw], charged, enear, sp, sq);
                                 } else {
                                     s_mk[wp][j >> 5][lane] |= 1u << (j & 31);
                                 }
@@ -295,26 +308,34 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                     ++ri;
                     ty = runs[ri].y;
                     rnext = runs[ri + 1].x;
-                    sg = s_sig2[as * nt + ty];
-                    ep = s_eps4[as * nt + ty];
+                    sg = __ldg(b.sig2 + as * nt + ty);
+                    ep = __ldg(b.eps4 + as * nt + ty);
                     ljB = ep * (sg * sg * sg);
                     ljA = ljB * (sg * sg * sg);
                 }
                 if (!PQ) {
-                    // the marked pairs in FP64, lanes in step (each takes its next marked entry)
+                    // the marked pairs in FP64, lanes in step: each lane takes its next marked entry
+                    // of the chunk (in entry order), so the warp takes as many steps as the lane
+                    // with the most marks
                     const double2 pxy = s_p64[wp][lane][0], pzz = s_p64[wp][lane][1];
-                    const double skq = s_site64[as].w;
+                    const double skq = s_site64[as].w, alpha64 = b.alphas[fw];
+                    const double* sig2 = b.sig2_64 + as * nt;
+                    const double* eps4 = b.eps4_64 + as * nt;
                     float dsp = 0.f, dsq = 0.f;
-#pragma unroll 1
-                    for (int32_t q = 0; q < PA_CHUNK32 / 32; ++q) {
-                        uint32_t mq = s_mk[wp][q][lane];
-                        while (__any_sync(FULL, mq != 0)) {
-                            if (mq != 0) {
-                                const int32_t e = base + q * 32 + __ffs(mq) - 1;
-                                mq &= mq - 1;
-                                pair64<false>(b, e, pxy.x, pxy.y, pzz.x, as, b.list_type[e], skq, fw, charged, enear,
-                                              dsp, dsq);
-                            }
+                    int32_t left = 0;
+#pragma unroll
+                    for (int q = 0; q < PA_CHUNK32 / 32; ++q) left += __popc(s_mk[wp][q][lane]);
+                    int32_t q = 0;
+                    uint32_t mq = s_mk[wp][0][lane];
+                    while (__any_sync(FULL, left > 0)) {
+                        if (left > 0) {
+                            while (mq == 0) mq = s_mk[wp][++q][lane];  // a mark is left: ends by word 3
+                            const int32_t e = base + q * 32 + __ffs(mq) - 1;
+                            mq &= mq - 1;
+                            --left;
+                            const int32_t te = b.list_type[e];
+                            pair64<false>(b.list_xyzq64, b.rl2_64, b.re2_64, e, pxy.x, pxy.y, pzz.x,
+                                          make_double2(sig2[te], eps4[te]), skq, alpha64, charged, enear, dsp, dsq);
                         }
                     }
                 }
