@@ -46,6 +46,91 @@ struct DevMem {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// The FP32 screened Coulomb term beyond the near radius in the exp-free form
+// erfc(alpha r)/r = exp(-alpha^2 r^2) u H(u), u = 1/r^2, H(u) = r erfcx(alpha r): H as a polynomial
+// of PA_NHP coefficients in x = k1 u + k0 (x in [-1, 1] on [u_lo, u_hi]), fitted by relative least
+// squares at HPOLY_NODES Chebyshev nodes (Householder QR in FP64). The fit is accepted when,
+// evaluated as the kernel does (FP32 coefficients, FP32 fma Horner at an FP32 u), it stays within
+// HPOLY_TOL of H (relative) at HPOLY_CHECK + 1 points; otherwise the kernel keeps the rational form.
+constexpr int HPOLY_NODES = 64;
+constexpr int HPOLY_CHECK = 4000;
+constexpr double HPOLY_TOL = 1.5e-7;
+struct HPolyFit {
+    bool ok = false;
+    float k1 = 0.f, k0 = 0.f;
+    float c[PA_NHP] = {};
+    double err = 0;
+};
+double erfcx_host(double z) { return std::erfc(z) * std::exp(z * z); }
+HPolyFit fit_hpoly(double alpha, double ulo, double uhi) {
+    HPolyFit f;
+    constexpr int M = HPOLY_NODES, D = PA_NHP;
+    if (!(alpha > 0) || !(ulo > 0) || !(uhi > ulo)) return f;
+    double A[M][D], y[M];
+    const double pi = 3.14159265358979323846;
+    for (int i = 0; i < M; ++i) {
+        const double x = std::cos(pi * (i + 0.5) / M);
+        const double u = ulo + (x + 1) * (uhi - ulo) / 2;
+        const double r = 1 / std::sqrt(u);
+        const double h = r * erfcx_host(alpha * r);
+        if (!(std::isfinite(h) && h > 0)) return f;
+        double xp = 1;
+        for (int j = 0; j < D; ++j) { A[i][j] = xp / h; xp *= x; }
+        y[i] = 1;
+    }
+    // Householder QR of A, applied to y as well; then R c = (Q^T y)[0:D]
+    for (int k = 0; k < D; ++k) {
+        double nrm = 0;
+        for (int i = k; i < M; ++i) nrm += A[i][k] * A[i][k];
+        nrm = std::sqrt(nrm);
+        if (!(nrm > 0)) return f;
+        const double ak = A[k][k] > 0 ? -nrm : nrm;
+        double v[M];
+        for (int i = k; i < M; ++i) v[i] = A[i][k];
+        v[k] -= ak;
+        double vv = 0;
+        for (int i = k; i < M; ++i) vv += v[i] * v[i];
+        if (!(vv > 0)) continue;
+        for (int j = k; j < D; ++j) {
+            double t = 0;
+            for (int i = k; i < M; ++i) t += v[i] * A[i][j];
+            t = 2 * t / vv;
+            for (int i = k; i < M; ++i) A[i][j] -= t * v[i];
+        }
+        double t = 0;
+        for (int i = k; i < M; ++i) t += v[i] * y[i];
+        t = 2 * t / vv;
+        for (int i = k; i < M; ++i) y[i] -= t * v[i];
+    }
+    double c[D];
+    for (int k = D - 1; k >= 0; --k) {
+        double t = y[k];
+        for (int j = k + 1; j < D; ++j) t -= A[k][j] * c[j];
+        c[k] = t / A[k][k];
+    }
+    f.k1 = float(2 / (uhi - ulo));
+    f.k0 = float(-(uhi + ulo) / (uhi - ulo));
+    for (int j = 0; j < D; ++j) f.c[j] = float(c[j]);
+    double err = 0;
+    for (int i = 0; i <= HPOLY_CHECK; ++i) {
+        const float uf = float(ulo + (uhi - ulo) * i / double(HPOLY_CHECK));
+        const float x = std::fmaf(uf, f.k1, f.k0);
+        float p = f.c[D - 1];
+        for (int j = D - 2; j >= 0; --j) p = std::fmaf(p, x, f.c[j]);
+        const double r = 1 / std::sqrt(double(uf));
+        const double e = std::fabs(double(p) / (r * erfcx_host(alpha * r)) - 1);
+        err = std::isfinite(e) ? std::max(err, e) : HUGE_VAL;
+    }
+    f.err = err;
+    f.ok = err <= HPOLY_TOL;
+    return f;
+}
+// The fit of the last (alpha, u_lo, u_hi) a context used.
+struct HPolyCache {
+    double alpha = -1, ulo = 0, uhi = 0;
+    HPolyFit fit;
+};
+
 }  // namespace
 
 struct PendingTiming { int cls, n; cudaEvent_t a, b; };
@@ -89,6 +174,7 @@ struct pa_context {
     // launch choices, the replayable graph of the last call's device sequence and its key
     pa_tuning tuning{0.0, 0, 0};
     pa_fp32_split split{PA_DEFAULT_NEAR_RADIUS, 1, 0};
+    mutable HPolyCache hpoly;  // the exp-free screened-Coulomb fit of the last split applied
     cudaGraphExec_t gexec = nullptr;
     std::vector<unsigned char> gkey, last_key;  // key of the captured graph, and of the last call
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
@@ -146,6 +232,7 @@ struct pa_batch {
     std::vector<int32_t> kn_h;         // 3*nk integer coefficients
     std::vector<int32_t> kstep_h;      // nfw: row step in n3
     double guest_qabs = 0;             // Σ |guest charge|
+    double alpha_common = 0;           // the frameworks' common Ewald alpha (0: they differ)
     std::vector<int32_t> ncells_h;     // 3*nfw cell-list grid
     std::vector<double> const_offset_h;  // nfw constant offsets (pair-table updates included)
     double cutoff = 0;                 // LJ cutoff
@@ -622,6 +709,9 @@ pa_status upload_impl(pa_context* ctx, const pa_batch_desc* desc, pa_batch* B) {
     std::vector<F> cells(9 * nfw), inv(9 * nfw);
     for (int i = 0; i < 9 * nfw; ++i) { cells[i] = F(desc->cells[i]); inv[i] = F(desc->invcells[i]); }
     std::vector<double> alphas(desc->alphas, desc->alphas + nfw), co(desc->constant_offset, desc->constant_offset + nfw);
+    B->alpha_common = nfw > 0 ? alphas[0] : 0.0;
+    for (int f = 1; f < nfw; ++f)
+        if (alphas[f] != alphas[0]) B->alpha_common = 0.0;
     std::vector<typename pa::Vec4<F>::T> atoms(na);
     std::vector<int32_t> types(na);
     for (int64_t j = 0; j < na; ++j) {
@@ -808,12 +898,17 @@ cudaError_t launch_energy(const pa_batch* B, const pa::DevBatch<float>& v32, con
     if (B->precision == PA_PRECISION_F32) {
         const int32_t per = (ctas >= 1 && ctas <= PA_CTAS_PER_SM32) ? ctas : PA_CTAS_PER_SM32;
         const unsigned grid = unsigned(num_sms * per), block = 32 * PA_WARPS32;
-        if (v32.rl2 == v32.re2) {
-            if (w.item_pq) pa::k_energy32<NS, true, true><<<grid, block, 0, st>>>(v32, ca, w);
-            else pa::k_energy32<NS, true, false><<<grid, block, 0, st>>>(v32, ca, w);
+        const bool eq = v32.rl2 == v32.re2, pq = w.item_pq != nullptr;
+        if (v32.hpoly) {
+            if (eq) { if (pq) pa::k_energy32<NS, true, true, true><<<grid, block, 0, st>>>(v32, ca, w);
+                      else pa::k_energy32<NS, true, false, true><<<grid, block, 0, st>>>(v32, ca, w); }
+            else { if (pq) pa::k_energy32<NS, false, true, true><<<grid, block, 0, st>>>(v32, ca, w);
+                   else pa::k_energy32<NS, false, false, true><<<grid, block, 0, st>>>(v32, ca, w); }
         } else {
-            if (w.item_pq) pa::k_energy32<NS, false, true><<<grid, block, 0, st>>>(v32, ca, w);
-            else pa::k_energy32<NS, false, false><<<grid, block, 0, st>>>(v32, ca, w);
+            if (eq) { if (pq) pa::k_energy32<NS, true, true, false><<<grid, block, 0, st>>>(v32, ca, w);
+                      else pa::k_energy32<NS, true, false, false><<<grid, block, 0, st>>>(v32, ca, w); }
+            else { if (pq) pa::k_energy32<NS, false, true, false><<<grid, block, 0, st>>>(v32, ca, w);
+                   else pa::k_energy32<NS, false, false, false><<<grid, block, 0, st>>>(v32, ca, w); }
         }
     } else {
         pa::k_energy64<NS><<<num_sms * 4, PA_TILE64, 0, st>>>(B->d64, ca, w);
@@ -863,9 +958,10 @@ cudaError_t launch_recip_combine(const pa::DevBatch<float>& v32, const pa::CallA
 // rounding bands around the cutoffs (4e-6 rc^2, several times the largest FP32 error of a squared
 // distance up to the cutoff: entries and sites relative to a bin centre within rc plus a bin's
 // circumradius carry at most half an ulp of a coordinate below 16 Å each).
-void apply_split(const pa_context* ctx, pa::DevBatch<float>& v) {
+void apply_split(const pa_context* ctx, const pa_batch* B, pa::DevBatch<float>& v) {
     const double rn = ctx->split.near_radius;
     v.rmode = ctx->split.fp64_reciprocal == 0 ? 0 : v.has_ksplit ? 2 : 1;
+    v.hpoly = 0;
     if (!(rn > 0)) {
         v.rn2 = 0.f;
         v.rl2_lo = v.rl2_hi = v.rl2;
@@ -876,6 +972,21 @@ void apply_split(const pa_context* ctx, pa::DevBatch<float>& v) {
     const double bl = 4.0e-6 * v.rl2_64, be = 4.0e-6 * v.re2_64;
     v.rl2_lo = float(v.rl2_64 - bl); v.rl2_hi = float(v.rl2_64 + bl);
     v.re2_lo = float(v.re2_64 - be); v.re2_hi = float(v.re2_64 + be);
+    // every FP32 Coulomb pair has rn^2 <= r^2 < re^2: the exp-free form when its fit on that
+    // range (widened by 1e-5 relative for FP32 rounding) is accurate enough
+    if (v.has_charge && B->alpha_common > 0 && rn * rn < v.re2_64) {
+        const double ulo = 1 / (v.re2_64 * (1 + 1e-5)), uhi = 1 / (rn * rn * (1 - 1e-5));
+        HPolyCache& hc = ctx->hpoly;
+        if (hc.alpha != B->alpha_common || hc.ulo != ulo || hc.uhi != uhi) {
+            hc.fit = fit_hpoly(B->alpha_common, ulo, uhi);
+            hc.alpha = B->alpha_common; hc.ulo = ulo; hc.uhi = uhi;
+        }
+        if (hc.fit.ok) {
+            v.hpoly = 1;
+            v.hk1 = hc.fit.k1; v.hk0 = hc.fit.k0;
+            for (int j = 0; j < PA_NHP; ++j) v.hc[j] = hc.fit.c[j];
+        }
+    }
 }
 
 template <typename F>
@@ -1279,7 +1390,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     // table) and pose-independent terms replace the batch's, plus the live guests' sites
     pa::DevBatch<float> v32;  // byte copy (padding included: the bytes key the CUDA graph)
     std::memcpy(&v32, &B->d32, sizeof(v32));
-    apply_split(ctx, v32);
+    apply_split(ctx, B, v32);
     pa::ChainArgs cargs{};
     int64_t ng = 0;
     if (chain) {
@@ -2157,7 +2268,7 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
         cudaError_t e = cudaSuccess;
         pa::DevBatch<float> v32;  // the context's FP32/FP64 pair split, as pa_widom applies it
         std::memcpy(&v32, &B->d32, sizeof(v32));
-        apply_split(ctx, v32);
+        apply_split(ctx, B, v32);
         if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, v32, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
         if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(v32, ca, w, ctx->num_sms, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));

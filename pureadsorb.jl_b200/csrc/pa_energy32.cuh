@@ -119,8 +119,10 @@ __device__ __forceinline__ void pair64(const double4* xyzq64, double rl2, double
 }
 
 // EQCUT: the LJ and Ewald cutoffs are equal, so one test selects both terms. PQ: also store each
-// item's LJ sums per type run (w.item_pq) for the adjoint.
-template <int NS, bool EQCUT, bool PQ>
+// item's LJ sums per type run (w.item_pq) for the adjoint. HP: the FP32 screened Coulomb term in
+// the exp-free form (b.hpoly; every FP32 pair lies beyond the near radius), otherwise as
+// exp(-z^2) P(t), t = 2/(2 + z), z = alpha r.
+template <int NS, bool EQCUT, bool PQ, bool HP>
 __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(DevBatch<float> b, CallArgs ca, Work w) {
     __shared__ __align__(128) float4 s_xyzq[PA_WARPS32][2][PA_CHUNK32];
     __shared__ __align__(8) uint64_t s_bar[PA_WARPS32][2];
@@ -255,7 +257,30 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                 continue;
                             }
                             float e = 0.f;
-                            if (charged) {
+                            if (HP && charged) {
+                                // u = 1/r^2 serves both terms: LJ, and exp(-alpha^2 r^2) u H(u)
+                                const float ri2 = rcp_nr(r2);
+                                if (EQCUT || r2 < rl2) {
+                                    if (PQ) {
+                                        const float x = sg * ri2;
+                                        const float x3 = x * x * x;
+                                        const float u = x3 * x3 - x3;
+                                        e = ep * u;
+                                        sp += u;
+                                        sq = fmaf(x3, x3, sq + u);
+                                    } else {
+                                        const float ri6 = ri2 * ri2 * ri2;
+                                        e = ri6 * fmaf(ljA, ri6, -ljB);
+                                    }
+                                }
+                                if (EQCUT || r2 < re2) {
+                                    const float x = fmaf(ri2, b.hk1, b.hk0);
+                                    float p = b.hc[PA_NHP - 1];
+#pragma unroll
+                                    for (int k = PA_NHP - 2; k >= 0; --k) p = fmaf(p, x, b.hc[k]);
+                                    e = fmaf(qk * at.w, p * ex2_ftz(r2 * a2n) * ri2, e);
+                                }
+                            } else if (charged) {
                                 // one reciprocal square root serves both terms: 1/r^2 = (1/r)^2
                                 float ri = rsqrt_ftz(r2);
                                 ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);

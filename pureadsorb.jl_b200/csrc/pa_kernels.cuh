@@ -23,6 +23,8 @@
 
 namespace pa {
 
+#define PA_NHP 8  // coefficients of the exp-free screened-Coulomb polynomial (degree 7)
+
 template <typename F> struct Vec4;
 template <> struct Vec4<float> { typedef float4 T; };
 template <> struct Vec4<double> { typedef double4 T; };
@@ -87,6 +89,12 @@ struct DevBatch {
     const int32_t* ks32_off;                      // nfw+1
     int32_t has_ksplit;
     F rl2_lo, rl2_hi, re2_lo, re2_hi;             // rounding bands around the cutoffs
+    // FP32 screened Coulomb beyond the near radius in the exp-free form (hpoly != 0):
+    // erfc(alpha r)/r = exp(-alpha^2 r^2) u H(u), u = 1/r^2, H a polynomial of PA_NHP coefficients
+    // hc in x = hk1 u + hk0 (fitted per call on the host for the batch's alpha and [1/re^2, 1/rn^2])
+    int32_t hpoly;
+    float hk1, hk0;
+    float hc[PA_NHP];
 };
 
 // Per-call arguments shared by the kernels.
@@ -403,7 +411,7 @@ __device__ __forceinline__ int32_t floor_div(int32_t x, int32_t n) { return x >=
 #define PA_P0_WARPS 8
 #define PA_P0_QMAX 64
 template <int NS>
-__global__ void __launch_bounds__(32 * PA_P0_WARPS, 3) k_phase0_32(DevBatch<float> b, CallArgs ca, Work w,
+__global__ void __launch_bounds__(32 * PA_P0_WARPS, 4) k_phase0_32(DevBatch<float> b, CallArgs ca, Work w,
                                                                   const int32_t* order, const float* rho2,
                                                                   const int32_t* reach0) {
     __shared__ float4 s_img[PA_P0_WARPS][32];          // staged atom images (x, y, z), packed cell
