@@ -30,7 +30,7 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM 
 # autotuner's choice), from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum); they
 # cannot be measured inside the bench
 # (with the default FP32/FP64 split)
-ENERGY32_TRAFFIC_BYTES = {3.0: 129.783040e6 + 10.789632e6}
+ENERGY32_TRAFFIC_BYTES = {3.0: 130.597376e6 + 10.378496e6, 3.5: 105.653504e6 + 8.462592e6}
 FP64_PEAK_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12  # TFLOP/s: 64 FP64 FMA lanes per SM
 # the metric and workload names of both arms (ours and the reference's CPU implementation)
 METRIC = "Widom insertions/s (CO2, 5,832-atom framework)"
@@ -631,14 +631,17 @@ def main():
         rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
         # executed work of k_energy32 per survivor (FMA = 2 flops): each of its N (insertion,
         # site) items walks its bin's list, 8 FP32 flops per entry for the distance; a pair in
-        # the cutoff takes 52 FP32 flops (LJ 10 + screened Coulomb 38 + compensated add 4), or,
-        # closer than the near radius, 54 FP64 flops (distance 8, LJ 7, screened Coulomb 38,
-        # sum 1). The bound is the FP32 flops at the FP32 FMA peak plus the FP64 flops at the
-        # FP64 peak; `achieved` is the FP32-equivalent rate (FP64 flops weighted by the peak
-        # ratio), so frac = that bound's time / the measured time. The reciprocal term
-        # (10 per (k, site) + 7 per k, 25 per (row start, site)) runs in its own kernel.
-        flops32 = 8 * N * L + 52 * (n_lj - n_near)
-        flops64 = 54 * n_near
+        # the cutoff takes, in FP32, 37 flops in the exp-free form (reciprocal 5, LJ 5, screened
+        # Coulomb 23, compensated add 4) or 52 in the rational one (LJ 10, screened Coulomb 38,
+        # compensated add 4), or, closer than the near radius, 59 FP64 flops (distance 8,
+        # reciprocal square root 10, LJ 7, screened Coulomb 33, sum 1). The bound is the FP32
+        # flops at the FP32 FMA peak plus the FP64 flops at the FP64 peak; `achieved` is the
+        # FP32-equivalent rate (FP64 flops weighted by the peak ratio), so frac = that bound's
+        # time / the measured time. The reciprocal term (10 per (k, site) + 7 per k, 25 per
+        # (row start, site)) runs in its own kernel.
+        exp_free, fit_err = ctx.fp32_form()
+        flops32 = 8 * N * L + (37 if exp_free else 52) * (n_lj - n_near)
+        flops64 = 59 * n_near
         peak = fp32_peak(torch)
         flops_surv = flops32 + flops64 * (peak / FP64_PEAK_NOMINAL)
         flops_recip = (10 * N + 7) * nk + 25 * N * rows
@@ -656,7 +659,8 @@ def main():
                 "flops_per_survivor_fp32_equivalent": flops_surv, "reciprocal_flops_per_survivor": flops_recip,
                 "reciprocal_combine_ms_per_step": kms[6] / args.steps, "reference_algorithm_flops_per_survivor": ref_alg,
                 "survivor_fraction": surv_frac, "list_entries_per_bin": L, "pairs_lj": n_lj, "pairs_ewald": n_ew,
-                "pairs_fp64": n_near}
+                "pairs_fp64": n_near, "fp32_coulomb_form": "exp-free" if exp_free else "rational",
+                "fp32_coulomb_fit_error": fit_err}
 
         # plain FP64 form on the same workload and stream (the >= 3x denominator)
         fp64 = None

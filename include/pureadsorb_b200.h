@@ -94,6 +94,14 @@ typedef struct pa_fp32_split {
 } pa_fp32_split;
 pa_status pa_context_set_fp32_split(pa_context* ctx, const pa_fp32_split* split);
 pa_status pa_context_get_fp32_split(const pa_context* ctx, pa_fp32_split* split);
+/* The form of the FP32 screened-Coulomb pairs in the context's last FP32 energy launch (pa_widom,
+ * pa_widom_grad or pa_widom_static): *exp_free = 1 when they were evaluated as
+ * exp(-alpha^2 r^2) u H(u), u = 1/r^2, with H a degree-7 polynomial fitted on the host for the
+ * batch's alpha over [1/rc^2, 1/near_radius^2] (used when every framework shares one alpha and the
+ * fit, evaluated in FP32 as the kernel does, stays within 1.5e-7 relative; *fit_error is that
+ * fit's largest relative error), 0 when they took the rational form exp(-z^2) P(t), t = 2/(2+z)
+ * (*fit_error = 0). Both 0 before any such launch. */
+pa_status pa_context_fp32_form(const pa_context* ctx, int32_t* exp_free, double* fit_error);
 
 /*
  * The fields of a `FrameworkBatch` (src/batch.jl:72-104), as raw arrays. natoms = Σ atoms

@@ -90,6 +90,7 @@ SIGNATURES = [
     ("pa_cell_sort", _i32, [_p, _p, _i64, _p, _p, _p]),
     ("pa_context_set_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
     ("pa_context_get_fp32_split", _i32, [_p, ctypes.POINTER(Fp32Split)]),
+    ("pa_context_fp32_form", _i32, [_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]),
     ("pa_batch_upload", _i32, [_p, ctypes.POINTER(BatchDesc), _i32, ctypes.POINTER(_p)]),
     ("pa_batch_free", _i32, [_p]),
     ("pa_batch_set_pair_tables", _i32, [_p, _p, _p, _p, _p]),
@@ -226,6 +227,14 @@ class Context:
         sp = Fp32Split()
         self.check(lib().pa_context_get_fp32_split(self.handle, ctypes.byref(sp)), "pa_context_get_fp32_split")
         return sp
+
+    def fp32_form(self):
+        """(exp_free, fit_error) of the last FP32 energy launch: whether its FP32 screened-Coulomb
+        pairs took the exp-free form exp(-alpha^2 r^2) u H(u), and the accepted fit's largest
+        relative error (pa_context_fp32_form)."""
+        ef, err = ctypes.c_int32(0), ctypes.c_double(0.0)
+        self.check(lib().pa_context_fp32_form(self.handle, ctypes.byref(ef), ctypes.byref(err)), "pa_context_fp32_form")
+        return bool(ef.value), float(err.value)
 
     def kernel_times(self):
         ms = np.zeros(8)

@@ -175,6 +175,8 @@ struct pa_context {
     pa_tuning tuning{0.0, 0, 0};
     pa_fp32_split split{PA_DEFAULT_NEAR_RADIUS, 1, 0};
     mutable HPolyCache hpoly;  // the exp-free screened-Coulomb fit of the last split applied
+    int32_t last_hpoly = 0;    // the form of the last FP32 energy launch (pa_context_fp32_form)
+    double last_hpoly_err = 0;
     cudaGraphExec_t gexec = nullptr;
     std::vector<unsigned char> gkey, last_key;  // key of the captured graph, and of the last call
     // device copies of seed and kT read by the kernels, pinned staging of the segment sums and
@@ -1118,6 +1120,13 @@ pa_status pa_context_get_fp32_split(const pa_context* ctx, pa_fp32_split* split)
     return PA_OK;
 }
 
+pa_status pa_context_fp32_form(const pa_context* ctx, int32_t* exp_free, double* fit_error) {
+    if (!ctx || !exp_free || !fit_error) return PA_ERR_ARG;
+    *exp_free = ctx->last_hpoly;
+    *fit_error = ctx->last_hpoly ? ctx->last_hpoly_err : 0.0;
+    return PA_OK;
+}
+
 pa_status pa_context_get_tuning(const pa_context* ctx, pa_tuning* t) {
     if (!ctx || !t) return PA_ERR_ARG;
     *t = ctx->tuning;
@@ -1391,6 +1400,7 @@ pa_status pa_widom(pa_context* ctx, const pa_batch* B, const pa_widom_args* args
     pa::DevBatch<float> v32;  // byte copy (padding included: the bytes key the CUDA graph)
     std::memcpy(&v32, &B->d32, sizeof(v32));
     apply_split(ctx, B, v32);
+    if (B->precision == PA_PRECISION_F32) { ctx->last_hpoly = v32.hpoly; ctx->last_hpoly_err = ctx->hpoly.fit.err; }
     pa::ChainArgs cargs{};
     int64_t ng = 0;
     if (chain) {
@@ -2269,6 +2279,7 @@ extern "C" pa_status pa_widom_static(pa_context* ctx, const pa_batch* B, const p
         pa::DevBatch<float> v32;  // the context's FP32/FP64 pair split, as pa_widom applies it
         std::memcpy(&v32, &B->d32, sizeof(v32));
         apply_split(ctx, B, v32);
+        if (B->precision == PA_PRECISION_F32) { ctx->last_hpoly = v32.hpoly; ctx->last_hpoly_err = ctx->hpoly.fit.err; }
         if (e == cudaSuccess) { PA_DISPATCH_NS(N, (e = launch_energy<NSV>(B, v32, ca, f32 ? wi : w, ctx->num_sms, ctx->tuning.ctas_per_sm, st))); }
         if (e == cudaSuccess && f32) { PA_DISPATCH_NS(N, (e = launch_recip_combine<NSV>(v32, ca, w, ctx->num_sms, st))); }
         if (e != cudaSuccess) return fail(ctx, PA_ERR_CUDA, std::string("energy kernel launch: ") + cudaGetErrorString(e));

@@ -82,6 +82,9 @@ def test_poses_flags_energies_co2(pa, orc, backend, co2_small, T):
             assert r.K_H_err == pytest.approx(q.K_H_err, rel=1e-8)
             assert abs(r.q_st_err - q.q_st_err) <= 1e-10 * (abs(q.q_st) + q.q_st_err)
     else:
+        # the default split on this workload evaluates its FP32 Coulomb pairs in the exp-free form
+        exp_free, fit_err = backend.ctx.fp32_form()
+        assert exp_free and 0 < fit_err <= 1.5e-7
         err = np.abs(a - b)
         assert np.all(within_f32(a, b)), f"{int(np.sum(~within_f32(a, b)))} outside, max err {err.max()}"
         for r, q in zip(res, ref_results(pa, batch, ref, kT, 4)):
@@ -138,6 +141,7 @@ def test_fp32_all_pairs_mode(pa, orc, backend, case):
     ctx.set_fp32_split(near_radius=0.0, fp64_reciprocal=False)
     try:
         res, ins, ref, kT = run_both(pa, orc, batch, guest, 20_000, 11, 4, backend=backend)
+        assert ctx.fp32_form() == (False, 0.0)  # no near radius: the rational form
     finally:
         ctx.set_fp32_split(near_radius=old.near_radius, fp64_reciprocal=old.fp64_reciprocal)
     assert np.array_equal(ins["flags"], ref["flags"])
@@ -147,6 +151,24 @@ def test_fp32_all_pairs_mode(pa, orc, backend, case):
     for r, q in zip(res, ref_results(pa, batch, ref, kT, 4)):
         assert abs(math.log(r.K_H) - math.log(q.K_H)) <= 1e-3
         assert abs(r.q_st - q.q_st) <= 5.18e-4
+
+
+def test_rational_form_when_the_fit_is_refused(pa, orc, backend, co2_small):
+    # a 4 Å near radius widens the exp-free fit's range until it misses 1.5e-7 at this alpha: the
+    # FP32 Coulomb pairs take the rational form, within the all-FP32 bound (pairs at 4-6 Å in FP32)
+    fws, ff, guest, ewald = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32)
+    ctx = backend.ctx
+    old = ctx.fp32_split()
+    ctx.set_fp32_split(near_radius=4.0)
+    try:
+        res, ins, ref, kT = run_both(pa, orc, batch, guest, 20_000, 13, 4, backend=backend)
+        assert ctx.fp32_form() == (False, 0.0)
+    finally:
+        ctx.set_fp32_split(near_radius=old.near_radius, fp64_reciprocal=old.fp64_reciprocal)
+    surv = ref["flags"] == 0
+    a, b = ins["dU"][surv], ref["dU"][surv]
+    assert np.all(np.abs(a - b) <= FAST_REL * np.abs(b) + FAST_ABS)
 
 
 def test_empty_box_ideal_gas(pa, backend):
