@@ -8,9 +8,11 @@
 // independent warps; each warp streams its bin's imaged neighbour list (positions relative to the
 // bin centre, charge, type) through its own two shared-memory stages with cp.async.bulk copies
 // completing on its own mbarriers, so warps never wait for one another. FP32 Lennard-Jones +
-// screened Coulomb inside the cutoffs with a compensated sum per item.
+// screened Coulomb inside the cutoffs, each pair's term added exactly to an FP64 sum per item;
+// pairs closer than the near radius, or at a cutoff's rounding band, are marked during the walk
+// and evaluated in FP64 after each chunk.
 //
-// k_recip32: the reciprocal cross term per insertion, over tiles of 32 insertions of one bin:
+// k_recip: the reciprocal cross term per insertion, over tiles of 32 insertions of one bin:
 // per-bin FP64 phase factors, then cos/sin recurrences along k-vector rows per lane.
 //
 // k_combine (pa_kernels.cuh) adds the site sums, the reciprocal term and the constant offset in a
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
         const float NLOG2E = -1.4426950408889634f;
         const float a2n = (alpha * alpha) * NLOG2E;  // exp(-alpha^2 r^2) = 2^(r^2 a2n)
         const float halpha = 0.5f * alpha;
-        float esum = 0.f, ecmp = 0.f;  // compensated real-space sum
+        double eacc = 0.0;  // the FP32 pairs' terms, each added exactly to an FP64 sum
         // LJ parameters of the current host type for this lane's site: list entries come in runs of
         // one type (the bin's run table), the same for every lane, so the loop runs uniformly from
         // one run boundary to the next and reloads them there
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                                     e = ri6 * fmaf(ljA, ri6, -ljB);
                                 }
                             }
-                            kahan_add(esum, ecmp, e);
+                            eacc += double(e);
                         }
                     }
                     if (j >= n) break;
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
             return;
         }
         if (PQ && active && nch > 0) runsums[ri] = make_float2(sp, sq);  // the last run
-        if (active) w.dUs[it] = (double(esum) - double(ecmp)) + enear;
+        if (active) w.dUs[it] = eacc + enear;
     }
 }
 
