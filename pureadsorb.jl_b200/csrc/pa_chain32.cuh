@@ -2,7 +2,7 @@
 // src/nvt.jl:85-124): the guest-guest real-space term of each test insertion.
 //
 // The host-guest terms of such an insertion are the FP32 path's own kernels (k_energy32 for the
-// real space, k_recip32 against the system's running structure factor host + guests, which the
+// real space, k_recip against the system's running structure factor host + guests, which the
 // call substitutes for the host's), and k_combine adds this kernel's term and the system's
 // pose-independent constant. Here: for every live guest j of the insertion's system and every
 // site pair (a of the test guest, b of guest j), one minimum image of the site-site vector
@@ -10,8 +10,8 @@
 // KE q_a q_b erfc(alpha r)/r inside the Ewald cutoff, with a compensated sum per lane and a
 // fixed-order FP64 warp reduction. The geometry (test sites, site-site vectors, images, r^2) is
 // FP64: the sites are absolute Cartesian positions across the cell, whose FP32 differences would
-// lose about 1e-7 of the cell length; r^2 is then rounded once and the pair terms use k_energy32's
-// FP32 arithmetic.
+// lose about 1e-7 of the cell length; r^2 is then rounded once and the pair terms use the FP32
+// arithmetic of k_energy32's rational form (guest-guest pairs have no near radius).
 //
 // One warp per insertion, lanes over the (live guest, guest site) pairs of the system (a system
 // holds tens of guests, so lanes over guests alone would leave most of the warp idle). Included by
