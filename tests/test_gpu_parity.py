@@ -153,6 +153,21 @@ def test_fp32_all_pairs_mode(pa, orc, backend, case):
         assert abs(r.q_st - q.q_st) <= 5.18e-4
 
 
+@pytest.mark.parametrize("cutoff,precision", [(10.0, 1e-5), (14.0, 1e-7)])
+def test_exp_free_form_other_ewald_settings(pa, orc, backend, co2_small, cutoff, precision):
+    # an Ewald cutoff below and above the LJ one (the unequal-cutoff kernels) and other alphas: the
+    # exp-free fit is accepted and every survivor meets the per-insertion criterion
+    fws, ff, guest, _ = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, pa.EwaldParams(cutoff, precision), T=np.float32)
+    res, ins, ref, kT = run_both(pa, orc, batch, guest, 20_000, 9, 4, backend=backend)
+    exp_free, fit_err = backend.ctx.fp32_form()
+    assert exp_free and 0 < fit_err <= 1.5e-7
+    assert np.array_equal(ins["flags"], ref["flags"])
+    surv = ref["flags"] == 0
+    a, b = ins["dU"][surv], ref["dU"][surv]
+    assert np.all(within_f32(a, b)), f"{int(np.sum(~within_f32(a, b)))} outside"
+
+
 def test_rational_form_when_the_fit_is_refused(pa, orc, backend, co2_small):
     # a 4 Å near radius widens the exp-free fit's range until it misses 1.5e-7 at this alpha: the
     # FP32 Coulomb pairs take the rational form, within the all-FP32 bound (pairs at 4-6 Å in FP32)
