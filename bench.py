@@ -30,7 +30,11 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM 
 # autotuner's choice), from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum); they
 # cannot be measured inside the bench
 # (with the default FP32/FP64 split)
-ENERGY32_TRAFFIC_BYTES = {3.0: 130.597376e6 + 10.378496e6, 3.5: 105.653504e6 + 8.462592e6}
+ENERGY32_TRAFFIC_BYTES = {3.0: 130.084864e6 + 9.805568e6, 3.5: 105.290752e6 + 10.230016e6}
+# Warp instructions of one k_energy32 launch on this workload (smsp__inst_executed.sum from the same
+# captures): the issue-slot roofline divides them by the launch's CUDA-event time
+ENERGY32_INSTRUCTIONS = {3.0: 1523469529, 3.5: 1566257192}
+ISSUE_PER_CYCLE = 148 * 4  # one warp instruction per cycle per SM sub-partition
 FP64_PEAK_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12  # TFLOP/s: 64 FP64 FMA lanes per SM
 # the metric and workload names of both arms (ours and the reference's CPU implementation)
 METRIC = "Widom insertions/s (CO2, 5,832-atom framework)"
@@ -649,9 +653,22 @@ def main():
         surv_per_launch = surv_frac * (s1 - s0) * (ninsert / nseg)
         achieved = flops_surv * surv_per_launch / (e_ms / 1e3) / 1e12
         ref_alg = (30 * 5832 + 8 * N * 5832 + 11 * n_lj + 36 * n_ew + 15 * N * nk + 4 * nk)
+        # the issue-slot roofline: the kernel's warp instructions (ncu, this workload and bin width)
+        # per second against one per cycle per SM sub-partition at the SM clock sampled while timing
+        ncu_workload = args.ninsert == 1_000_000 and world == 1 and rn == 6.0
+        n_inst = ENERGY32_INSTRUCTIONS.get(float(tune.bin_width)) if ncu_workload else None
+        sm_mhz = clk.summary().get("sm_mhz") or 1965.0
+        issue = None
+        if n_inst is not None:
+            ach = n_inst / (e_ms / 1e3) / 1e9
+            pk = ISSUE_PER_CYCLE * sm_mhz * 1e6 / 1e9
+            issue = {"instructions": n_inst, "achieved": ach, "peak": pk, "unit": "Ginst/s", "frac": ach / pk,
+                     "note": "warp instructions per launch from ncu (smsp__inst_executed.sum) on this workload and "
+                             "bin width; peak one warp instruction per cycle per SM sub-partition at the sampled "
+                             "SM clock"}
         roof = {"bound": "fp32+fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": ENERGY32_TRAFFIC_BYTES.get(float(tune.bin_width))
-                if (args.ninsert == 1_000_000 and world == 1 and rn == 6.0) else None,
+                "traffic": ENERGY32_TRAFFIC_BYTES.get(float(tune.bin_width)) if ncu_workload else None,
+                "issue": issue,
                 "kernel": "k_energy32", "kernel_ms_per_launch": e_ms,
                 "peak_note": "nominal FP32 FMA peak at the maximum SM clock (148 SMs x 128 lanes x 2 x 1.965 GHz); "
                              "FP64 flops weighted by FP32/FP64 nominal peaks (74.4 / 37.2 TFLOP/s)",
