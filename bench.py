@@ -635,17 +635,17 @@ def main():
         rows = 1 + int(np.sum(~((kc[1:, 0] == kc[:-1, 0]) & (kc[1:, 1] == kc[:-1, 1])))) if nk else 0
         # executed work of k_energy32 per survivor (FMA = 2 flops): each of its N (insertion,
         # site) items walks its bin's list, 8 FP32 flops per entry for the distance; a pair in
-        # the cutoff takes, in FP32, 33 flops in the exp-free form (reciprocal 5, LJ 5, screened
+        # the cutoff takes, in FP32, 29 flops in the exp-free form (reciprocal 1, LJ 5, screened
         # Coulomb 23) or 48 in the rational one (LJ 10, screened Coulomb 38), plus one FP64 add
-        # into the item's sum, or, closer than the near radius, 59 FP64 flops (distance 8,
-        # reciprocal square root 10, LJ 7, screened Coulomb 33, sum 1). The bound is the FP32
+        # into the item's sum, or, closer than the near radius, 55 FP64 flops (distance 8,
+        # reciprocal square root 6, LJ 7, screened Coulomb 33, sum 1). The bound is the FP32
         # flops at the FP32 FMA peak plus the FP64 flops at the FP64 peak; `achieved` is the
         # FP32-equivalent rate (FP64 flops weighted by the peak ratio), so frac = that bound's
         # time / the measured time. The reciprocal term (10 per (k, site) + 7 per k, 25 per
         # (row start, site)) runs in its own kernel.
         exp_free, fit_err = ctx.fp32_form()
-        flops32 = 8 * N * L + (33 if exp_free else 48) * (n_lj - n_near)
-        flops64 = 59 * n_near + (n_lj - n_near)
+        flops32 = 8 * N * L + (29 if exp_free else 48) * (n_lj - n_near)
+        flops64 = 55 * n_near + (n_lj - n_near)
         peak = fp32_peak(torch)
         flops_surv = flops32 + flops64 * (peak / FP64_PEAK_NOMINAL)
         flops_recip = (10 * N + 7) * nk + 25 * N * rows

@@ -36,16 +36,15 @@ __device__ __forceinline__ float ex2_ftz(float x) {
     return r;
 }
 
-// 1/sqrt(x) in FP64, x > 0 and normal: the hardware approximation (rsqrt.approx.ftz.f64) refined
-// by two steps of Newton's iteration y <- y (3/2 - (x/2) y^2), each of which squares the relative
-// error; a few ulp from 1/sqrt(x).
+// 1/sqrt(x) in FP64, x > 0 and normal: the hardware approximation (rsqrt.approx.ftz.f64, measured
+// within 9.3e-7 relative on [1e-2, 1e4] on the B200) refined by one step of Newton's iteration
+// y <- y (3/2 - (x/2) y^2), which squares the relative error: within 1.3e-12 (measured), about
+// 1e-11 eV on the largest near-pair terms.
 __device__ __forceinline__ double rsqrt64(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     const double h = 0.5 * x;
-    y = y * fma(-h * y, y, 1.5);
-    y = y * fma(-h * y, y, 1.5);
-    return y;
+    return y * fma(-h * y, y, 1.5);
 }
 
 // S(u) = erf(sqrt u)/sqrt u on 0 <= u <= PA_ERFS64_UMAX from the PA_ERFS64 polynomial (Horner).
@@ -260,8 +259,11 @@ __global__ void __launch_bounds__(32 * PA_WARPS32, PA_CTAS_PER_SM32) k_energy32(
                             }
                             float e = 0.f;
                             if (HP && charged) {
-                                // u = 1/r^2 serves both terms: LJ, and exp(-alpha^2 r^2) u H(u)
-                                const float ri2 = rcp_nr(r2);
+                                // u = 1/r^2 serves both terms: LJ, and exp(-alpha^2 r^2) u H(u); the
+                                // hardware reciprocal (about 1 ulp) without a Newton step: every pair
+                                // here lies beyond the near radius, where its terms are small
+                                float ri2;
+                                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ri2) : "f"(r2));
                                 if (EQCUT || r2 < rl2) {
                                     if (PQ) {
                                         const float x = sg * ri2;

@@ -52,6 +52,8 @@ def test_batched_frameworks_against_oracle_same_poses(pa, orc, backend):
     np.maximum.at(xmax, sysid, x)
     heavy = x >= xmax[sysid] - 50
     o = np.argsort(-np.abs(a - r))[:8]
+    ratio = np.abs(a - r) / np.maximum(1e-5 * np.abs(r), 8.62e-8)
+    print(f"\nworst survivor at {ratio.max():.3f} of the per-insertion tolerance")
     print(f"\nper-insertion: {int(bad.sum())} of {len(r)} survivors outside the tolerance, {int((bad & heavy).sum())} of "
           f"{int(heavy.sum())} heavy; worst (ref dU, dev - ref, heavy): "
           + ", ".join(f"({r[i]:.4g}, {a[i] - r[i]:.2e}, {bool(heavy[i])})" for i in o)
