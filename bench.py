@@ -30,10 +30,10 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM 
 # autotuner's choice), from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum); they
 # cannot be measured inside the bench
 # (with the default FP32/FP64 split)
-ENERGY32_TRAFFIC_BYTES = {3.0: 130.084864e6 + 9.805568e6, 3.5: 105.290752e6 + 10.230016e6}
+ENERGY32_TRAFFIC_BYTES = {3.0: 130.300928e6 + 9.088256e6, 3.5: 105.949696e6 + 8.178432e6}
 # Warp instructions of one k_energy32 launch on this workload (smsp__inst_executed.sum from the same
 # captures): the issue-slot roofline divides them by the launch's CUDA-event time
-ENERGY32_INSTRUCTIONS = {3.0: 1523469529, 3.5: 1566257192}
+ENERGY32_INSTRUCTIONS = {3.0: 1469443993, 3.5: 1513756043}
 ISSUE_PER_CYCLE = 148 * 4  # one warp instruction per cycle per SM sub-partition
 FP64_PEAK_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12  # TFLOP/s: 64 FP64 FMA lanes per SM
 # the metric and workload names of both arms (ours and the reference's CPU implementation)
