@@ -387,6 +387,23 @@ __global__ void __launch_bounds__(256) k_draw32(DevBatch<float> b, CallArgs ca, 
 }
 
 __device__ __forceinline__ int32_t floor_div(int32_t x, int32_t n) { return x >= 0 ? x / n : -((n - 1 - x) / n); }
+// x / d and x % d for 0 <= x < 2^22 and d >= 1, from the FP32 estimate x * rd (rd = 1/d rounded):
+// its error is below one unit there, so one correction each way makes it exact.
+__device__ __forceinline__ int32_t div_small(int32_t x, int32_t d, float rd, int32_t& rem) {
+    int32_t q = int32_t(float(x) * rd);
+    int32_t r = x - q * d;
+    if (r < 0) { --q; r += d; } else if (r >= d) { ++q; r -= d; }
+    rem = r;
+    return q;
+}
+// floor(x / n) for a cell index x of a region around the grid [0, n): -1, 0 or 1 without a
+// division when -n <= x < 2n
+__device__ __forceinline__ int32_t wrap_of(int32_t x, int32_t n) {
+    if (x >= 0 && x < n) return 0;
+    if (x < 0 && x >= -n) return -1;
+    if (x >= n && x < 2 * n) return 1;
+    return floor_div(x, n);
+}
 
 // k_phase0_32: one warp scans the hard core of 32 consecutive insertions of `order` together.
 // The warp's insertions lie in one or two centre sub-bins, so their per-site stencils (the cells
@@ -538,6 +555,7 @@ __global__ void __launch_bounds__(32 * PA_P0_WARPS, 4) k_phase0_32(DevBatch<floa
         const int32_t nt = b.ntypes;
         const int32_t E0 = hi[0] - lo[0] + 1, E1 = hi[1] - lo[1] + 1;
         const int32_t ncell = E0 * E1 * (hi[2] - lo[2] + 1);
+        const float rE0 = 1.0f / float(E0), rE1 = 1.0f / float(E1);
         // decide the queued pairs, one lane each
         const auto flush = [&](int32_t qn) {
             __syncwarp();
@@ -589,12 +607,20 @@ __global__ void __launch_bounds__(32 * PA_P0_WARPS, 4) k_phase0_32(DevBatch<floa
             float Wx = 0.f, Wy = 0.f, Wz = 0.f;
             uint32_t cpk = 0u;
             if (pi < ncell) {
-                const int32_t u[3] = {lo[0] + pi % E0, lo[1] + (pi / E0) % E1, lo[2] + pi / (E0 * E1)};
+                int32_t u[3];
+                if (ncell < (1 << 22)) {
+                    int32_t r0, r1;
+                    const int32_t q0 = div_small(pi, E0, rE0, r0);
+                    const int32_t q1 = div_small(q0, E1, rE1, r1);
+                    u[0] = lo[0] + r0; u[1] = lo[1] + r1; u[2] = lo[2] + q1;
+                } else {
+                    u[0] = lo[0] + pi % E0; u[1] = lo[1] + (pi / E0) % E1; u[2] = lo[2] + pi / (E0 * E1);
+                }
                 int32_t cc[3];
                 float wv[3];
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
-                    const int32_t wr = floor_div(u[r], n[r]);
+                    const int32_t wr = wrap_of(u[r], n[r]);
                     cc[r] = u[r] - wr * n[r];
                     wv[r] = float(wr);
                 }
