@@ -186,6 +186,27 @@ def test_rational_form_when_the_fit_is_refused(pa, orc, backend, co2_small):
     assert np.all(np.abs(a - b) <= FAST_REL * np.abs(b) + FAST_ABS)
 
 
+def test_every_pair_in_fp64_when_the_near_radius_exceeds_the_cutoff(pa, orc, backend, co2_small):
+    # a 13 Å near radius (cutoffs 12 Å) sends every in-cutoff pair through the FP64 pass: no FP32
+    # Coulomb pairs are left (the form query reports the rational form, unused), and every survivor
+    # lies far inside the per-insertion criterion (the FP32 rows of the reciprocal term remain)
+    fws, ff, guest, ewald = co2_small
+    batch = pa.FrameworkBatch(fws, ff, guest, ewald, T=np.float32)
+    ctx = backend.ctx
+    old = ctx.fp32_split()
+    ctx.set_fp32_split(near_radius=13.0)
+    try:
+        res, ins, ref, kT = run_both(pa, orc, batch, guest, 20_000, 17, 4, backend=backend)
+        assert ctx.fp32_form() == (False, 0.0)
+    finally:
+        ctx.set_fp32_split(near_radius=old.near_radius, fp64_reciprocal=old.fp64_reciprocal)
+    assert np.array_equal(ins["flags"], ref["flags"])
+    surv = ref["flags"] == 0
+    a, b = ins["dU"][surv], ref["dU"][surv]
+    ratio = np.abs(a - b) / np.maximum(F32_REL * np.abs(b), F32_ABS)
+    assert ratio.max() <= 0.25, ratio.max()
+
+
 def test_empty_box_ideal_gas(pa, backend):
     A = pa.cell_matrix(30.0, 30.0, 30.0, 90, 90, 90)
     fw = pa.Framework(A, np.zeros((0, 3)), [], [], np.zeros(0))
